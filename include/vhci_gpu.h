@@ -1,0 +1,177 @@
+/*
+ * vhci_gpu.h — C ABI of the B200 (sm_100a) heat-bath VCI + Epstein-Nesbet PT2 library.
+ *
+ * The reference program (berkelbach-group/VHCI) is one C++ binary with global state and no plugin
+ * or FFI layer.  This ABI exposes, as plain C calls over host pointers and sizes, the internal
+ * seams of that program; each declaration names the reference function it stands in for.  The
+ * `vhci` command-line tool (drop-in for `vhci -n/-i/-o/-c`) and the Python harness (ctypes) are
+ * both written on top of it.
+ *
+ * Conventions
+ *  - Every call returns a vhci_status (0 = OK).  vhci_last_error() gives the message.
+ *  - The caller owns every host buffer; the context owns all device memory and one CUDA stream.
+ *  - A context is used by one host thread at a time; separate contexts may run concurrently.
+ *  - There is no CPU fallback: without a usable CUDA device, vhci_create* returns VHCI_E_CUDA.
+ *  - Basis states are passed as rows of per-mode quanta, uint8_t[n * nmodes], row-major.
+ *  - Eigenvectors are passed column-major, double[n * k] (column j = state j), as the reference's
+ *    Eigen MatrixXd.
+ */
+#ifndef VHCI_GPU_H
+#define VHCI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int vhci_status;
+enum {
+  VHCI_OK = 0,
+  VHCI_E_INPUT = 1,         /* malformed input file / arguments (reference: message + exit)     */
+  VHCI_E_OOM = 2,           /* device memory exhausted                                           */
+  VHCI_E_TABLE_FULL = 3,    /* a device hash table could not take a key within its probe bound   */
+  VHCI_E_KEY_OVERFLOW = 4,  /* a state needs more than 255 quanta in one mode                    */
+  VHCI_E_NOT_CONVERGED = 5, /* eigensolver hit its iteration limit (reference: Ham.cpp:367-368)  */
+  VHCI_E_CUDA = 6,          /* CUDA runtime / library failure                                    */
+  VHCI_E_STATE = 7,         /* call made in the wrong state (e.g. no vectors yet)                */
+  VHCI_E_NEG_ZPE = 8        /* zero-point energy < 0 (reference: VHCI.cpp:122-137)               */
+};
+
+typedef struct vhci_ctx vhci_ctx;
+
+/* Options.  Fill with vhci_default_opts() and change fields as needed. */
+typedef struct {
+  int device;          /* CUDA device ordinal                                                   */
+  int precision;       /* 0: FP64 throughout (parity path); 1: mixed — FP32 Hamiltonian values
+                          with FP64 accumulation, FP64 Ritz steps, PT2 denominators and a final
+                          FP64 residual sweep                                                    */
+  double eig_tol;      /* relative residual tolerance, reference 1e-10 (Ham.cpp:363)            */
+  int eig_maxit;       /* eigensolver iteration bound, reference 1000 (Ham.cpp:363)             */
+  int verbose;         /* 1: print the reference's progress lines to stdout                    */
+  int host_threads;    /* host threads for host-side steps (reference -n)                       */
+  int64_t pt2_chunk;   /* max perturber-Hamiltonian entries held at once (0 = automatic)        */
+  int structural_nnz;  /* 1: also count the reference's structural Hamiltonian entries for the
+                          "% sparse" log line (Ham.cpp:341-342); costs one extra pass           */
+} vhci_opts;
+
+/* Problem description in memory (the content of a reference input file, Input_Reader.cpp). */
+typedef struct {
+  int nmodes;               /* Nm                                                              */
+  const double* freq;       /* [nmodes] harmonic frequencies (cm^-1)                           */
+  const int* cap;           /* [nmodes] per-mode quanta cap of the initial basis               */
+  int max_quanta;           /* Ntot: initial basis = all states with sum of quanta <= Ntot     */
+  int nfc;                  /* number of anharmonic force constants                            */
+  const int* fc_order;      /* [nfc] order 3..6                                                */
+  const int* fc_modes;      /* [nfc * 6] mode indices (first fc_order[i] used)                 */
+  const double* fc_value;   /* [nfc] unscaled values as written in the input file              */
+  double eps1;              /* HCI_Eps (0 = conventional VCI over the initial basis)           */
+  int nstate;               /* Nstate                                                          */
+  int pt2;                  /* PT2 flag                                                        */
+  double eps2;              /* PT2_Eps (0 = every connected state)                             */
+} vhci_problem;
+
+typedef struct {
+  int nmodes, nstate, pt2, key_bits, key_words;
+  double eps1, eps2;
+  int64_t n_basis;          /* current variational basis size                                  */
+  int64_t n_fc, n_hb;       /* scaled FCs; heat-bath list (FCs + aggregated singles/doubles)   */
+  int64_t n_groups;         /* distinct quanta-change patterns of the FC list (H connections)  */
+  int64_t n_vectors;        /* eigenpairs currently held                                       */
+  int64_t h_nnz;            /* stored off-diagonal Hamiltonian entries (0 if not built)        */
+} vhci_info;
+
+/* Per-phase device time of the most recent solve (milliseconds) and work counters. */
+typedef struct {
+  double ms_select, ms_hbuild, ms_eigs, ms_pt2, ms_total;
+  double ms_spmm;                 /* part of ms_eigs spent in the SpMM kernel                  */
+  int64_t spmm_calls, spmm_cols;  /* SpMM launches and total vector columns multiplied         */
+  int64_t spmm_bytes;             /* algorithmic bytes of all SpMM launches                    */
+  int64_t hbuild_probes;          /* hash probes issued by the Hamiltonian build               */
+  int64_t select_candidates;      /* candidate states generated by heat-bath selection         */
+  int64_t pt2_entries;            /* perturber-Hamiltonian entries (a, i, H_ai)                */
+  int64_t pt2_perturbers;         /* |P|                                                       */
+  double ms_pt2_reduce;           /* part of ms_pt2 spent in the fused EN reduction kernel     */
+  int64_t pt2_reduce_bytes;       /* algorithmic bytes of the EN reduction                     */
+  int eig_iterations;             /* Davidson iterations summed over all eigensolves           */
+  int hci_iterations;
+} vhci_stats;
+
+typedef void (*vhci_iter_cb)(void* user, int iteration, int64_t n_basis, double zpe);
+
+void vhci_default_opts(vhci_opts* o);
+
+/* Parse an input file with the reference's positional rules (Input_Reader.cpp:170-291), scale
+ * the FCs (ScaleFC, :494-515), build the heat-bath list (:366-460, HB.cpp:17-22) and the initial
+ * basis (:295-364), and upload everything.  restart != 0 starts from the ground state only, as
+ * the reference does before reading a checkpoint (:296-307). */
+vhci_status vhci_create_from_file(const char* path, const vhci_opts* o, int restart,
+                                  vhci_ctx** out);
+/* Same from an in-memory problem. */
+vhci_status vhci_create(const vhci_problem* p, const vhci_opts* o, int restart, vhci_ctx** out);
+vhci_status vhci_destroy(vhci_ctx* c);
+vhci_status vhci_last_error(const vhci_ctx* c, char* buf, size_t n);
+vhci_status vhci_get_info(const vhci_ctx* c, vhci_info* info);
+vhci_status vhci_get_stats(const vhci_ctx* c, vhci_stats* s);
+vhci_status vhci_reset_stats(vhci_ctx* c);
+
+/* Scaled FC list in input order and the sorted heat-bath list: value plus up to 6 (mode, power)
+ * pairs (mode -1 pads).  Parity dumps of Input_Reader.cpp:249-291,366-460 and HB.cpp:17-22. */
+vhci_status vhci_get_fc_list(const vhci_ctx* c, double* value, int32_t* modes, int32_t* powers);
+vhci_status vhci_get_hb_list(const vhci_ctx* c, double* value, int32_t* modes, int32_t* powers);
+/* Harmonic frequencies as parsed. */
+vhci_status vhci_get_freqs(const vhci_ctx* c, double* freq);
+
+/* Basis I/O (the reference's BasisSet).  set_basis replaces the basis and drops vectors. */
+vhci_status vhci_set_basis(vhci_ctx* c, const uint8_t* quanta, int64_t n);
+vhci_status vhci_get_basis(const vhci_ctx* c, uint8_t* quanta, int64_t cap, int64_t* n);
+
+/* Eigenpairs (the reference's Evecs/Evals).  set_vectors injects caller vectors (n x k,
+ * column-major) for selection/PT2 known-answer tests; get_vectors copies k of them out. */
+vhci_status vhci_set_vectors(vhci_ctx* c, const double* C, const double* E, int k);
+vhci_status vhci_get_vectors(const vhci_ctx* c, double* C, double* E, int k);
+
+/* Heat-bath selection, AddStatesHB over all states (HB.cpp:24-174, driver :198-223) with
+ * Cmax over the first min(nstate, n) vector columns.  append != 0 appends the new states (in
+ * ascending key order) and updates the device hash; otherwise they are kept for
+ * vhci_get_selected().  n_new receives the number of new states. */
+vhci_status vhci_select(vhci_ctx* c, double eps, int append, int64_t* n_new);
+vhci_status vhci_get_selected(const vhci_ctx* c, uint8_t* quanta, int64_t cap, int64_t* n);
+
+/* Sparse Hamiltonian over the current basis (MakeHamSparse, Ham.cpp:203-344), kept on device.
+ * nnz receives the stored entry count including the diagonal. */
+vhci_status vhci_build_h(vhci_ctx* c, int64_t* nnz);
+/* Copy the Hamiltonian out as CSR with columns ascending in every row (nnz from build_h). */
+vhci_status vhci_get_h_csr(const vhci_ctx* c, int64_t* rowptr, int32_t* col, double* val);
+/* Structural entry count of the reference's pair loop (every pair passing its quanta gates),
+ * for the "% sparse" line (Ham.cpp:341-342). */
+vhci_status vhci_structural_nnz(vhci_ctx* c, int64_t* nnz);
+
+/* Lowest k eigenpairs of the current Hamiltonian (SparseDiagonalize, Ham.cpp:347-370; dense
+ * eigensolve for small bases, DenseDiagonalize, :372-379).  Vectors stay on device; E (k)
+ * receives the eigenvalues if not NULL. */
+vhci_status vhci_eigs(vhci_ctx* c, int k, double* E);
+
+/* Full heat-bath procedure (Perform_HCI, HB.cpp:176-265) or, for eps1 == 0, one eigensolve over
+ * the initial basis (VHCI.cpp:49-76).  checkpoint_path may be NULL; when given, a checkpoint is
+ * written after each iteration whose basis exceeds 1e5 states (HB.cpp:250-262). */
+vhci_status vhci_hci(vhci_ctx* c, const char* checkpoint_path, vhci_iter_cb cb, void* user);
+
+/* Epstein-Nesbet PT2 (DoPT2, PT2.cpp:16-154) over the current vectors.  dE (min(nstate, n))
+ * receives the corrections, which are also added to the held eigenvalues.  n_pert receives |P|. */
+vhci_status vhci_pt2(vhci_ctx* c, double eps2, double* dE, int64_t* n_pert);
+
+/* Frequency/assignment file (PrintFreqs, Ham.cpp:448-502). */
+vhci_status vhci_write_freqs(const vhci_ctx* c, const char* path);
+/* Checkpoint text file (WriteCheckpoint / ReadCheckpoint, Core_functions.cpp:94-167). */
+vhci_status vhci_write_checkpoint(const vhci_ctx* c, const char* path);
+vhci_status vhci_read_checkpoint(vhci_ctx* c, const char* path);
+
+/* Eigenvalues currently held (n <= k). */
+vhci_status vhci_get_energies(const vhci_ctx* c, double* E, int k, int* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VHCI_GPU_H */

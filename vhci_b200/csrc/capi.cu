@@ -1,0 +1,655 @@
+// C ABI core: context lifetime, key layout, device tables, basis/vectors I/O, heat-bath
+// selection and the Hamiltonian build.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "internal.h"
+
+namespace vhci {
+
+int fail(vhci_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(vhci_ctx* c, cudaError_t e, const char* where) {
+  cudaGetLastError();
+  const int code = (e == cudaErrorMemoryAllocation) ? VHCI_E_OOM : VHCI_E_CUDA;
+  return fail(c, code, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+int blas_fail(vhci_ctx* c, int st, const char* where) {
+  return fail(c, VHCI_E_CUDA, std::string(where) + ": library status " + std::to_string(st));
+}
+
+HashView basis_view(vhci_ctx* c) { return HashView{c->hslots.p, c->hmask, c->keys.p}; }
+
+ConnDev conn_view(vhci_ctx* c) {
+  ConnDev d;
+  d.groups = c->groups.p;
+  d.wdelta = c->wdelta.p;
+  d.ngroups = (int64_t)c->conn.groups.size();
+  d.terms = c->terms.p;
+  d.dterms = c->dterms.p;
+  d.ndterms = (int)c->conn.diag_terms.size();
+  d.T = c->T.p;
+  d.freq = c->freq.p;
+  d.nm = c->M.nm;
+  return d;
+}
+
+HBTable hb_view(vhci_ctx* c) {
+  return HBTable{c->hbdev.p, c->hbabs.p, c->hbcumd.p, (int)c->hbe.size()};
+}
+
+float event_ms(vhci_ctx* c) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
+  return ms;
+}
+
+int read_flags(vhci_ctx* c, int* flags) {
+  int h = 0;
+  VCK(cudaMemcpyAsync(&h, c->flags.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  VCK(cudaMemsetAsync(c->flags.p, 0, sizeof(int), c->st));
+  VCK(cudaStreamSynchronize(c->st));
+  *flags = h;
+  return VHCI_OK;
+}
+
+static KeyLayout make_layout(int nm, int bits) {
+  KeyLayout L;
+  L.bits = bits;
+  L.mpw = 64 / bits;
+  L.W = (nm + L.mpw - 1) / L.mpw;
+  L.qmax = (1 << bits) - 1;
+  return L;
+}
+
+template <class T>
+static int upload(vhci_ctx* c, DBuf<T>& b, const std::vector<T>& h) {
+  VCK(b.reserve(std::max<size_t>(h.size(), 1), c->st));
+  if (!h.empty())
+    VCK(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->st));
+  return VHCI_OK;
+}
+
+// Layout-dependent tables (packed key deltas, ladder factors) and the layout-free ones.
+int upload_tables(vhci_ctx* c) {
+  const KeyLayout& L = c->L;
+  std::vector<GroupDev> g(c->conn.groups.size());
+  std::vector<int64_t> wd(c->conn.groups.size() * L.W, 0);
+  for (size_t u = 0; u < g.size(); ++u) {
+    const Group& s = c->conn.groups[u];
+    GroupDev d{};
+    d.tb = s.term_begin;
+    d.te = s.term_end;
+    d.nchg = (uint8_t)s.nchg;
+    for (int k = 0; k < s.nchg; ++k) {
+      d.mode[k] = (uint8_t)s.mode[k];
+      d.delta[k] = (int8_t)s.delta[k];
+      const int w = s.mode[k] / L.mpw;
+      wd[u * L.W + w] += (int64_t)((uint64_t)(int64_t)s.delta[k] << ((s.mode[k] % L.mpw) * L.bits));
+    }
+    g[u] = d;
+  }
+  auto conv = [](const std::vector<Term>& in) {
+    std::vector<TermDev> out(in.size());
+    for (size_t i = 0; i < in.size(); ++i) {
+      TermDev t{};
+      t.fc = in[i].fc;
+      t.nk = in[i].nk;
+      for (int k = 0; k < kMaxOrder; ++k) {
+        t.mode[k] = in[i].mode[k];
+        t.pw[k] = in[i].pw[k];
+        t.dl[k] = in[i].dl[k];
+      }
+      out[i] = t;
+    }
+    return out;
+  };
+  std::vector<double> T;
+  ladder_table(L.qmax, T);
+  std::vector<HBDev> hb(c->hbe.size());
+  std::vector<double> habs(c->hbe.size());
+  for (size_t i = 0; i < hb.size(); ++i) {
+    HBDev d{};
+    d.zero_idx = c->hbe[i].zero_idx;
+    d.nk = (uint8_t)c->hbe[i].nk;
+    for (int k = 0; k < c->hbe[i].nk; ++k) {
+      d.mode[k] = (uint8_t)c->hbe[i].modes[k];
+      d.pw[k] = (uint8_t)c->hbe[i].powers[k];
+    }
+    hb[i] = d;
+    habs[i] = c->hbe[i].absfc;
+  }
+  VTRY(upload(c, c->groups, g));
+  VTRY(upload(c, c->wdelta, wd));
+  VTRY(upload(c, c->terms, conv(c->conn.terms)));
+  VTRY(upload(c, c->dterms, conv(c->conn.diag_terms)));
+  VTRY(upload(c, c->T, T));
+  VTRY(upload(c, c->freq, c->M.freq));
+  VTRY(upload(c, c->hbdev, hb));
+  VTRY(upload(c, c->hbabs, habs));
+  VTRY(upload(c, c->hbcumd, c->hbcum));
+  return VHCI_OK;
+}
+
+// Hash capacity for n_total keys at load <= 1/2; rebuilds the table when it grows.
+int ensure_hash(vhci_ctx* c, int64_t n_total) {
+  uint64_t need = 1024;
+  while (need < (uint64_t)(2 * n_total)) need <<= 1;
+  if (c->hmask + 1 >= need && c->hslots.p) return VHCI_OK;
+  VCK(c->hslots.reserve(need, c->st));
+  c->hmask = need - 1;
+  hash_clear(c->hslots.p, need, c->st);
+  hash_insert_range(c->hslots.p, c->hmask, c->keys.p, 0, c->n, c->L.W, c->flags.p, c->st);
+  return VHCI_OK;
+}
+
+int append_keys(vhci_ctx* c, const uint64_t* dkeys, int64_t m) {
+  if (m <= 0) return VHCI_OK;
+  const int64_t n1 = c->n + m;
+  if ((uint64_t)n1 >= 0xFFFFFFF0ull) return fail(c, VHCI_E_OOM, "basis exceeds 2^32 states");
+  VCK(c->keys.reserve((size_t)n1 * c->L.W, c->st, true));
+  VCK(cudaMemcpyAsync(c->keys.p + (size_t)c->n * c->L.W, dkeys, sizeof(uint64_t) * m * c->L.W,
+                      cudaMemcpyDeviceToDevice, c->st));
+  const int64_t n0 = c->n;
+  c->n = n1;
+  uint64_t need = 1024;
+  while (need < (uint64_t)(2 * n1)) need <<= 1;
+  if (c->hmask + 1 >= need) {
+    hash_insert_range(c->hslots.p, c->hmask, c->keys.p, n0, n1, c->L.W, c->flags.p, c->st);
+  } else {
+    c->hmask = 0;
+    VTRY(ensure_hash(c, n1));
+  }
+  c->h_valid = false;
+  return VHCI_OK;
+}
+
+// Re-encode every key with 8-bit mode fields (a state reached more than 15 quanta in a mode).
+int promote_layout(vhci_ctx* c) {
+  if (c->L.bits == 8) return fail(c, VHCI_E_KEY_OVERFLOW, "a state needs more than 255 quanta in one mode");
+  const KeyLayout A = c->L, B = make_layout(c->M.nm, 8);
+  if (B.W > 8) return fail(c, VHCI_E_INPUT, "too many modes for the 8-bit key layout (max 64)");
+  DBuf<uint64_t> nk;
+  VCK(nk.reserve(std::max<int64_t>(c->keys.cap / A.W * B.W, (int64_t)c->n * B.W + 16), c->st));
+  repack_keys(c->keys.p, A, nk.p, B, c->n, c->M.nm, c->st);
+  c->keys.release(c->st);
+  c->keys = nk;
+  if (c->nsel > 0 && c->sel.p) {
+    DBuf<uint64_t> ns;
+    VCK(ns.reserve((size_t)c->nsel * B.W, c->st));
+    repack_keys(c->sel.p, A, ns.p, B, c->nsel, c->M.nm, c->st);
+    c->sel.release(c->st);
+    c->sel = ns;
+  }
+  c->L = B;
+  VTRY(upload_tables(c));
+  c->hmask = 0;
+  VTRY(ensure_hash(c, c->n));
+  return VHCI_OK;
+}
+
+// ------------------------------------------------------------------ heat-bath selection ----
+
+int generate_new_set(vhci_ctx* c, double eps) {
+  if (c->nvec < 1 || c->x_rows != c->n)
+    return fail(c, VHCI_E_STATE, "selection needs eigenvectors over the current basis");
+  const int64_t n = c->n;
+  const int nopt = (int)std::min<int64_t>(std::min<int64_t>(c->M.nstate, n), c->nvec);
+  VCK(c->d64a.reserve(n, c->st));
+  VCK(c->i64a.reserve(n + 1, c->st));
+  VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(n), 1), c->st));
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    cmax_rows(c->X.p, n, c->ldx, nopt, c->d64a.p, c->st);
+    select_count(c->d64a.p, n, hb_view(c), eps, c->i64a.p, c->st);
+    exclusive_scan(c->i64a.p, c->i64a.p, n, c->scan_tmp.p, c->st);
+    int64_t total = 0;
+    VCK(cudaMemcpyAsync(&total, c->i64a.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+    VCK(cudaStreamSynchronize(c->st));
+    c->stats.select_candidates += total;
+    c->nsel = 0;
+    if (total == 0) return VHCI_OK;
+    // candidate capacity: grows on overflow, never beyond the work count
+    int64_t cap = std::min<int64_t>(total, std::max<int64_t>(4 * n, 1 << 22));
+    bool promoted = false;
+    for (;;) {
+      uint64_t slots = 1024;
+      while (slots < (uint64_t)(2 * cap)) slots <<= 1;
+      const int W = c->L.W;
+      VCK(c->u64a.reserve((size_t)cap * W, c->st));
+      VCK(c->u64b.reserve(slots, c->st));
+      VCK(c->u8a.reserve(cap, c->st));
+      VCK(c->ull.reserve(2, c->st));
+      VCK(cudaMemsetAsync(c->u8a.p, 0, cap, c->st));
+      VCK(cudaMemsetAsync(c->ull.p, 0, 2 * sizeof(unsigned long long), c->st));
+      hash_clear(c->u64b.p, slots, c->st);
+      NewSetView ns{c->u64b.p, slots - 1, c->u64a.p, c->u8a.p, c->ull.p, (uint64_t)cap, c->flags.p};
+      select_generate(c->keys.p, n, c->i64a.p, total, hb_view(c), c->L, basis_view(c), ns, c->st);
+      int fl = 0;
+      VTRY(read_flags(c, &fl));
+      if (fl & kFlagKeyOverflow) {
+        VTRY(promote_layout(c));
+        promoted = true;
+        break;
+      }
+      if (fl & (kFlagCandOverflow | kFlagTableFull)) {
+        if (cap >= total) return fail(c, VHCI_E_TABLE_FULL, "candidate set overflow");
+        cap = std::min<int64_t>(total, cap * 4);
+        continue;
+      }
+      unsigned long long ncand = 0;
+      VCK(cudaMemcpyAsync(&ncand, c->ull.p, sizeof(ncand), cudaMemcpyDeviceToHost, c->st));
+      VCK(cudaStreamSynchronize(c->st));
+      ncand = std::min<unsigned long long>(ncand, (unsigned long long)cap);
+      VCK(c->sel.reserve((size_t)std::max<unsigned long long>(ncand, 1) * W, c->st));
+      newset_compact(c->u64a.p, c->u8a.p, (int64_t)ncand, W, c->sel.p, c->ull.p + 1, c->st);
+      unsigned long long m = 0;
+      VCK(cudaMemcpyAsync(&m, c->ull.p + 1, sizeof(m), cudaMemcpyDeviceToHost, c->st));
+      VCK(cudaStreamSynchronize(c->st));
+      c->nsel = (int64_t)m;
+      if (m > 1) {
+        VCK(c->u64b.reserve((size_t)m * W, c->st));
+        VCK(c->scan_tmp.reserve(std::max<int64_t>(radix_hist_elems((int64_t)m), 1), c->st));
+        radix_sort_keys(c->sel.p, c->u64b.p, (int64_t)m, W, c->L.bits * c->M.nm,
+                        c->scan_tmp.p, c->st);
+      }
+      return VHCI_OK;
+    }
+    if (!promoted) break;
+  }
+  return fail(c, VHCI_E_KEY_OVERFLOW, "selection could not settle a key layout");
+}
+
+// --------------------------------------------------------------------- Hamiltonian build ----
+
+int build_h(vhci_ctx* c) {
+  const int64_t n = c->n;
+  VCK(cudaEventRecord(c->ev_a, c->st));
+  VCK(c->rowcnt.reserve(n, c->st));
+  VCK(c->rowptr.reserve(n + 1, c->st));
+  VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(n), 1), c->st));
+  hbuild_count(c->keys.p, n, c->L, basis_view(c), conn_view(c), c->rowcnt.p, c->st);
+  exclusive_scan_i32(c->rowcnt.p, c->rowptr.p, n, c->scan_tmp.p, c->st);
+  int64_t nnz = 0;
+  VCK(cudaMemcpyAsync(&nnz, c->rowptr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+  VCK(cudaStreamSynchronize(c->st));
+  VCK(c->col.reserve(std::max<int64_t>(nnz, 1), c->st));
+  if (c->o.precision == 1) {
+    VCK(c->valf.reserve(std::max<int64_t>(nnz, 1), c->st));
+  } else {
+    VCK(c->val.reserve(std::max<int64_t>(nnz, 1), c->st));
+  }
+  VCK(c->diag.reserve(n, c->st));
+  hbuild_fill(c->keys.p, n, c->L, basis_view(c), conn_view(c), c->rowptr.p, c->col.p,
+              c->o.precision == 1 ? nullptr : c->val.p, c->o.precision == 1 ? c->valf.p : nullptr,
+              c->diag.p, c->st);
+  VCK(cudaEventRecord(c->ev_b, c->st));
+  VCK(cudaEventSynchronize(c->ev_b));
+  VCK(cudaGetLastError());
+  c->stats.ms_hbuild += event_ms(c);
+  c->stats.hbuild_probes += 2 * n * (int64_t)c->conn.groups.size();
+  c->nnz = nnz;
+  c->h_valid = true;
+  return VHCI_OK;
+}
+
+static int create_common(vhci_ctx* c, int restart) {
+  std::string err;
+  if (!finalize_model(c->M, restart != 0, err)) return fail(c, VHCI_E_INPUT, err);
+  build_conn_tables(c->M, c->conn);
+  build_hb_entries(c->M, c->hbe, c->hbcum);
+  int maxq = 0;
+  for (uint8_t q : c->M.init_basis) maxq = std::max<int>(maxq, q);
+  c->L = make_layout(c->M.nm, maxq > 15 ? 8 : 4);
+  if (c->L.W > 8 && c->L.bits == 4) return fail(c, VHCI_E_INPUT, "too many modes (max 128)");
+  if (c->L.W > 8) return fail(c, VHCI_E_INPUT, "too many modes for the 8-bit key layout (max 64)");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(c, VHCI_E_CUDA, "no CUDA device available (this library has no CPU path)");
+  if (c->o.device < 0 || c->o.device >= ndev) return fail(c, VHCI_E_CUDA, "bad device ordinal");
+  VCK(cudaSetDevice(c->o.device));
+  VCK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  VCK(cudaEventCreate(&c->ev_a));
+  VCK(cudaEventCreate(&c->ev_b));
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, c->o.device) == cudaSuccess) {
+      uint64_t thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
+  VBL(cublasCreate(&c->blas));
+  VBL(cublasSetStream(c->blas, c->st));
+  VBL(cusolverDnCreate(&c->sol));
+  VBL(cusolverDnSetStream(c->sol, c->st));
+  VCK(c->flags.reserve(4, c->st));
+  VCK(cudaMemsetAsync(c->flags.p, 0, 4 * sizeof(int), c->st));
+  VTRY(upload_tables(c));
+  // initial basis
+  const int64_t n0 = c->M.n0;
+  DBuf<uint8_t> q;
+  VCK(q.reserve(std::max<int64_t>(n0 * c->M.nm, 1), c->st));
+  VCK(cudaMemcpyAsync(q.p, c->M.init_basis.data(), n0 * c->M.nm, cudaMemcpyHostToDevice, c->st));
+  VCK(c->keys.reserve((size_t)std::max<int64_t>(n0, 16) * c->L.W, c->st));
+  pack_keys(q.p, n0, c->M.nm, c->L, c->keys.p, c->st);
+  q.release(c->st);
+  c->n = n0;
+  c->hmask = 0;
+  VTRY(ensure_hash(c, n0));
+  int fl = 0;
+  VTRY(read_flags(c, &fl));
+  if (fl) return fail(c, VHCI_E_INPUT, "duplicate states in the initial basis");
+  c->restart = restart;
+  return VHCI_OK;
+}
+
+}  // namespace vhci
+
+using namespace vhci;
+
+extern "C" {
+
+void vhci_default_opts(vhci_opts* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->precision = 0;
+  o->eig_tol = 1e-10;
+  o->eig_maxit = 1000;
+  o->verbose = 0;
+  o->host_threads = 1;
+  o->pt2_chunk = 0;
+  o->structural_nnz = 0;
+}
+
+vhci_status vhci_create_from_file(const char* path, const vhci_opts* o, int restart,
+                                  vhci_ctx** out) {
+  if (!out) return VHCI_E_INPUT;
+  *out = nullptr;
+  vhci_ctx* c = new vhci_ctx();
+  if (o) c->o = *o; else vhci_default_opts(&c->o);
+  std::string err;
+  int r = VHCI_OK;
+  if (!parse_input_file(path, c->M, err)) r = fail(c, VHCI_E_INPUT, err);
+  else r = create_common(c, restart);
+  *out = c;  // returned even on failure so vhci_last_error() can report; caller destroys
+  return r;
+}
+
+vhci_status vhci_create(const vhci_problem* p, const vhci_opts* o, int restart, vhci_ctx** out) {
+  if (!out) return VHCI_E_INPUT;
+  *out = nullptr;
+  vhci_ctx* c = new vhci_ctx();
+  if (o) c->o = *o; else vhci_default_opts(&c->o);
+  std::string err;
+  int r = VHCI_OK;
+  if (!model_from_problem(p, c->M, err)) r = fail(c, VHCI_E_INPUT, err);
+  else r = create_common(c, restart);
+  *out = c;
+  return r;
+}
+
+vhci_status vhci_destroy(vhci_ctx* c) {
+  if (!c) return VHCI_OK;
+  if (c->st) {
+    cudaStreamSynchronize(c->st);
+    c->keys.release(c->st); c->hslots.release(c->st);
+    c->groups.release(c->st); c->wdelta.release(c->st); c->terms.release(c->st);
+    c->dterms.release(c->st); c->T.release(c->st); c->freq.release(c->st);
+    c->hbdev.release(c->st); c->hbabs.release(c->st); c->hbcumd.release(c->st);
+    c->rowcnt.release(c->st); c->rowptr.release(c->st); c->col.release(c->st);
+    c->val.release(c->st); c->valf.release(c->st); c->diag.release(c->st);
+    c->X.release(c->st); c->sel.release(c->st); c->flags.release(c->st);
+    c->i64a.release(c->st); c->i64b.release(c->st); c->scan_tmp.release(c->st);
+    c->d64a.release(c->st); c->u64a.release(c->st); c->u64b.release(c->st);
+    c->u8a.release(c->st); c->ull.release(c->st); c->solver_work.release(c->st);
+    c->solver_info.release(c->st);
+    cudaStreamSynchronize(c->st);
+  }
+  if (c->blas) cublasDestroy(c->blas);
+  if (c->sol) cusolverDnDestroy(c->sol);
+  if (c->ev_a) cudaEventDestroy(c->ev_a);
+  if (c->ev_b) cudaEventDestroy(c->ev_b);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return VHCI_OK;
+}
+
+vhci_status vhci_last_error(const vhci_ctx* c, char* buf, size_t n) {
+  if (!c || !buf || n == 0) return VHCI_E_INPUT;
+  std::snprintf(buf, n, "%s", c->err.c_str());
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_info(const vhci_ctx* c, vhci_info* info) {
+  if (!c || !info) return VHCI_E_INPUT;
+  info->nmodes = c->M.nm;
+  info->nstate = c->M.nstate;
+  info->pt2 = c->M.pt2;
+  info->key_bits = c->L.bits;
+  info->key_words = c->L.W;
+  info->eps1 = c->M.eps1;
+  info->eps2 = c->M.eps2;
+  info->n_basis = c->n;
+  info->n_fc = (int64_t)c->M.fcs.size();
+  info->n_hb = (int64_t)c->M.hb.size();
+  info->n_groups = (int64_t)c->conn.groups.size();
+  info->n_vectors = std::min<int64_t>(c->nvec, std::min<int64_t>(c->M.nstate, c->n));
+  info->h_nnz = c->h_valid ? c->nnz : 0;
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_stats(const vhci_ctx* c, vhci_stats* s) {
+  if (!c || !s) return VHCI_E_INPUT;
+  *s = c->stats;
+  return VHCI_OK;
+}
+
+vhci_status vhci_reset_stats(vhci_ctx* c) {
+  if (!c) return VHCI_E_INPUT;
+  c->stats = vhci_stats{};
+  return VHCI_OK;
+}
+
+static void dump_fc(const std::vector<ForceConstant>& L, double* v, int32_t* m, int32_t* p) {
+  for (size_t i = 0; i < L.size(); ++i) {
+    v[i] = L[i].fc;
+    for (int k = 0; k < kMaxOrder; ++k) {
+      m[i * kMaxOrder + k] = k < L[i].nk ? L[i].modes[k] : -1;
+      p[i * kMaxOrder + k] = k < L[i].nk ? L[i].powers[k] : 0;
+    }
+  }
+}
+
+vhci_status vhci_get_fc_list(const vhci_ctx* c, double* v, int32_t* m, int32_t* p) {
+  if (!c || !v || !m || !p) return VHCI_E_INPUT;
+  dump_fc(c->M.fcs, v, m, p);
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_hb_list(const vhci_ctx* c, double* v, int32_t* m, int32_t* p) {
+  if (!c || !v || !m || !p) return VHCI_E_INPUT;
+  dump_fc(c->M.hb, v, m, p);
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_freqs(const vhci_ctx* c, double* f) {
+  if (!c || !f) return VHCI_E_INPUT;
+  std::copy(c->M.freq.begin(), c->M.freq.end(), f);
+  return VHCI_OK;
+}
+
+vhci_status vhci_set_basis(vhci_ctx* c, const uint8_t* quanta, int64_t n) {
+  if (!c || !quanta || n <= 0) return VHCI_E_INPUT;
+  int maxq = 0;
+  for (int64_t i = 0; i < n * c->M.nm; ++i) maxq = std::max<int>(maxq, quanta[i]);
+  if (maxq > c->L.qmax) {
+    c->n = 0;
+    VTRY(promote_layout(c));
+  }
+  DBuf<uint8_t> q;
+  VCK(q.reserve(n * c->M.nm, c->st));
+  VCK(cudaMemcpyAsync(q.p, quanta, n * c->M.nm, cudaMemcpyHostToDevice, c->st));
+  VCK(c->keys.reserve((size_t)n * c->L.W, c->st));
+  pack_keys(q.p, n, c->M.nm, c->L, c->keys.p, c->st);
+  q.release(c->st);
+  c->n = n;
+  c->hmask = 0;
+  VTRY(ensure_hash(c, n));
+  int fl = 0;
+  VTRY(read_flags(c, &fl));
+  c->h_valid = false;
+  c->nvec = 0;
+  c->x_rows = 0;
+  c->E.clear();
+  if (fl & kFlagDuplicate) return fail(c, VHCI_E_INPUT, "duplicate states in the basis");
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_basis(const vhci_ctx* c0, uint8_t* quanta, int64_t cap, int64_t* n) {
+  vhci_ctx* c = const_cast<vhci_ctx*>(c0);
+  if (!c || !n) return VHCI_E_INPUT;
+  *n = c->n;
+  if (!quanta) return VHCI_OK;
+  if (cap < c->n) return fail(c, VHCI_E_INPUT, "basis buffer too small");
+  DBuf<uint8_t> q;
+  VCK(q.reserve(std::max<int64_t>(c->n * c->M.nm, 1), c->st));
+  unpack_keys(c->keys.p, c->n, c->M.nm, c->L, q.p, c->st);
+  VCK(cudaMemcpyAsync(quanta, q.p, c->n * c->M.nm, cudaMemcpyDeviceToHost, c->st));
+  q.release(c->st);
+  VCK(cudaStreamSynchronize(c->st));
+  return VHCI_OK;
+}
+
+vhci_status vhci_set_vectors(vhci_ctx* c, const double* C, const double* E, int k) {
+  if (!c || !C || !E || k <= 0) return VHCI_E_INPUT;
+  const int64_t n = c->n;
+  std::vector<double> h((size_t)n * k);
+  for (int64_t i = 0; i < n; ++i)
+    for (int j = 0; j < k; ++j) h[(size_t)i * k + j] = C[(size_t)j * n + i];
+  VCK(c->X.reserve((size_t)n * k, c->st));
+  VCK(cudaMemcpyAsync(c->X.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  VCK(cudaStreamSynchronize(c->st));
+  c->ldx = k;
+  c->nvec = k;
+  c->x_rows = n;
+  c->E.assign(E, E + k);
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_vectors(const vhci_ctx* c0, double* C, double* E, int k) {
+  vhci_ctx* c = const_cast<vhci_ctx*>(c0);
+  if (!c) return VHCI_E_INPUT;
+  if (k > c->nvec || c->x_rows != c->n) return fail(c, VHCI_E_STATE, "fewer vectors held than requested");
+  const int64_t n = c->n;
+  if (C) {
+    std::vector<double> h((size_t)n * c->ldx);
+    VCK(cudaMemcpyAsync(h.data(), c->X.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    VCK(cudaStreamSynchronize(c->st));
+    for (int64_t i = 0; i < n; ++i)
+      for (int j = 0; j < k; ++j) C[(size_t)j * n + i] = h[(size_t)i * c->ldx + j];
+  }
+  if (E)
+    for (int j = 0; j < k; ++j) E[j] = c->E[j];
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_energies(const vhci_ctx* c, double* E, int k, int* n) {
+  if (!c || !n) return VHCI_E_INPUT;
+  const int held = (int)std::min<int64_t>((int64_t)c->E.size(), std::min<int64_t>(c->M.nstate, c->n));
+  *n = held;
+  if (E)
+    for (int j = 0; j < std::min(k, held); ++j) E[j] = c->E[j];
+  return VHCI_OK;
+}
+
+vhci_status vhci_select(vhci_ctx* c, double eps, int append, int64_t* n_new) {
+  if (!c) return VHCI_E_INPUT;
+  VCK(cudaEventRecord(c->ev_a, c->st));
+  VTRY(generate_new_set(c, eps));
+  if (append && c->nsel > 0) {
+    VTRY(append_keys(c, c->sel.p, c->nsel));
+    // vectors keep their old rows; new rows are zero-extended by the next eigensolve
+  }
+  VCK(cudaEventRecord(c->ev_b, c->st));
+  VCK(cudaEventSynchronize(c->ev_b));
+  c->stats.ms_select += event_ms(c);
+  int fl = 0;
+  VTRY(read_flags(c, &fl));
+  if (fl & kFlagTableFull) return fail(c, VHCI_E_TABLE_FULL, "basis hash full");
+  if (n_new) *n_new = c->nsel;
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_selected(const vhci_ctx* c0, uint8_t* quanta, int64_t cap, int64_t* n) {
+  vhci_ctx* c = const_cast<vhci_ctx*>(c0);
+  if (!c || !n) return VHCI_E_INPUT;
+  *n = c->nsel;
+  if (!quanta || c->nsel == 0) return VHCI_OK;
+  if (cap < c->nsel) return fail(c, VHCI_E_INPUT, "buffer too small");
+  DBuf<uint8_t> q;
+  VCK(q.reserve(c->nsel * c->M.nm, c->st));
+  unpack_keys(c->sel.p, c->nsel, c->M.nm, c->L, q.p, c->st);
+  VCK(cudaMemcpyAsync(quanta, q.p, c->nsel * c->M.nm, cudaMemcpyDeviceToHost, c->st));
+  q.release(c->st);
+  VCK(cudaStreamSynchronize(c->st));
+  return VHCI_OK;
+}
+
+vhci_status vhci_build_h(vhci_ctx* c, int64_t* nnz) {
+  if (!c) return VHCI_E_INPUT;
+  VTRY(build_h(c));
+  if (nnz) *nnz = c->nnz + c->n;
+  return VHCI_OK;
+}
+
+vhci_status vhci_get_h_csr(const vhci_ctx* c0, int64_t* rowptr, int32_t* col, double* val) {
+  vhci_ctx* c = const_cast<vhci_ctx*>(c0);
+  if (!c || !rowptr || !col || !val) return VHCI_E_INPUT;
+  if (!c->h_valid) return fail(c, VHCI_E_STATE, "Hamiltonian not built");
+  const int64_t n = c->n;
+  std::vector<int64_t> rp(n + 1);
+  std::vector<int32_t> cl(c->nnz);
+  std::vector<double> vl(c->nnz), dg(n);
+  VCK(cudaMemcpyAsync(rp.data(), c->rowptr.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+  if (c->nnz) {
+    VCK(cudaMemcpyAsync(cl.data(), c->col.p, c->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, c->st));
+    if (c->o.precision == 1) {
+      std::vector<float> vf(c->nnz);
+      VCK(cudaMemcpyAsync(vf.data(), c->valf.p, c->nnz * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+      VCK(cudaStreamSynchronize(c->st));
+      for (int64_t e = 0; e < c->nnz; ++e) vl[e] = vf[e];
+    } else {
+      VCK(cudaMemcpyAsync(vl.data(), c->val.p, c->nnz * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    }
+  }
+  VCK(cudaMemcpyAsync(dg.data(), c->diag.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  VCK(cudaStreamSynchronize(c->st));
+  int64_t pos = 0;
+  std::vector<std::pair<int32_t, double>> row;
+  for (int64_t i = 0; i < n; ++i) {
+    rowptr[i] = pos;
+    row.clear();
+    for (int64_t e = rp[i]; e < rp[i + 1]; ++e) row.push_back({cl[e], vl[e]});
+    row.push_back({(int32_t)i, dg[i]});
+    std::sort(row.begin(), row.end(),
+              [](const std::pair<int32_t, double>& a, const std::pair<int32_t, double>& b) {
+                return a.first < b.first;
+              });
+    for (auto& e : row) { col[pos] = e.first; val[pos] = e.second; ++pos; }
+  }
+  rowptr[n] = pos;
+  return VHCI_OK;
+}
+
+vhci_status vhci_structural_nnz(vhci_ctx* c, int64_t* nnz) {
+  if (!c || !nnz) return VHCI_E_INPUT;
+  return fail(c, VHCI_E_STATE, "structural count not available in this build");
+}
+
+}  // extern "C"

@@ -1,0 +1,376 @@
+// Host orchestration: Epstein-Nesbet PT2 (PT2.cpp:16-154), the heat-bath driver loop
+// (Perform_HCI, HB.cpp:176-265; VHCI.cpp:49-80) and the reference's output and checkpoint files
+// (PrintFreqs, Ham.cpp:448-502; Write/ReadCheckpoint, Core_functions.cpp:94-167).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+
+#include "internal.h"
+
+namespace vhci {
+
+int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
+  if (c->nvec < 1 || c->x_rows != c->n) return fail(c, VHCI_E_STATE, "PT2 needs eigenvectors");
+  cudaStream_t s = c->st;
+  cudaEvent_t t0, t1;
+  VCK(cudaEventCreate(&t0));
+  VCK(cudaEventCreate(&t1));
+  VCK(cudaEventRecord(t0, s));
+  const int64_t n = c->n;
+  const int nopt = (int)std::min<int64_t>(std::min<int64_t>(c->M.nstate, n), c->nvec);
+  // perturber space: heat-bath screened states outside the basis (PT2.cpp:29-50)
+  VTRY(generate_new_set(c, eps2));
+  const int64_t np = c->nsel;
+  const KeyLayout L = c->L;
+  std::vector<double> dE(nopt, 0.0);
+  c->stats.pt2_perturbers += np;
+  if (np > 0) {
+    // perturber keys and hash
+    DBuf<uint64_t> pkeys, pslots;
+    VCK(pkeys.reserve((size_t)np * L.W, s));
+    VCK(cudaMemcpyAsync(pkeys.p, c->sel.p, (size_t)np * L.W * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    uint64_t ns = 1024;
+    while (ns < (uint64_t)(2 * np)) ns <<= 1;
+    VCK(pslots.reserve(ns, s));
+    hash_clear(pslots.p, ns, s);
+    hash_insert_range(pslots.p, ns - 1, pkeys.p, 0, np, L.W, c->flags.p, s);
+    HashView pv{pslots.p, ns - 1, pkeys.p};
+    // entry counts per perturber row
+    DBuf<int32_t> acount;
+    DBuf<int64_t> arow, tmp;
+    VCK(acount.reserve(np, s));
+    VCK(arow.reserve(np + 1, s));
+    VCK(tmp.reserve(std::max<int64_t>(scan_tmp_elems(np), 1), s));
+    VCK(cudaMemsetAsync(acount.p, 0, np * sizeof(int32_t), s));
+    pt2_count(c->keys.p, n, L, pv, conn_view(c), 0, np, acount.p, s);
+    exclusive_scan_i32(acount.p, arow.p, np, tmp.p, s);
+    std::vector<int64_t> arow_h(np + 1);
+    VCK(cudaMemcpyAsync(arow_h.data(), arow.p, (np + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    VCK(cudaStreamSynchronize(s));
+    const int64_t total = arow_h[np];
+    c->stats.pt2_entries += total;
+    // chunk the perturber range so one chunk's entries fit the budget
+    size_t freeb = 0, totb = 0;
+    cudaMemGetInfo(&freeb, &totb);
+    int64_t budget = c->o.pt2_chunk > 0 ? c->o.pt2_chunk : (int64_t)(freeb * 0.6 / 12.0);
+    budget = std::max<int64_t>(budget, 1 << 20);
+    std::vector<int64_t> bounds{0};
+    while (bounds.back() < np) {
+      const int64_t a0 = bounds.back();
+      const int64_t lim = arow_h[a0] + budget;
+      int64_t a1 = std::upper_bound(arow_h.begin() + a0 + 1, arow_h.end(), lim) - arow_h.begin() - 1;
+      if (a1 <= a0) a1 = a0 + 1;
+      bounds.push_back(std::min(a1, np));
+    }
+    DBuf<int32_t> ecol;
+    DBuf<double> eval, part, dEd, Ed;
+    const int64_t maxchunk = [&] {
+      int64_t mx = 0;
+      for (size_t q = 1; q < bounds.size(); ++q)
+        mx = std::max(mx, arow_h[bounds[q]] - arow_h[bounds[q - 1]]);
+      return mx;
+    }();
+    VCK(ecol.reserve(std::max<int64_t>(maxchunk, 1), s));
+    VCK(eval.reserve(std::max<int64_t>(maxchunk, 1), s));
+    const int nblk = pt2_en_blocks();
+    VCK(part.reserve((size_t)nblk * nopt, s));
+    VCK(dEd.reserve(nopt, s));
+    VCK(Ed.reserve(nopt, s));
+    VCK(cudaMemsetAsync(dEd.p, 0, nopt * sizeof(double), s));
+    VCK(cudaMemcpyAsync(Ed.p, c->E.data(), nopt * sizeof(double), cudaMemcpyHostToDevice, s));
+    DBuf<int64_t> crow;
+    for (size_t q = 1; q < bounds.size(); ++q) {
+      const int64_t a0 = bounds[q - 1], a1 = bounds[q];
+      VCK(crow.reserve(a1 - a0 + 1, s));
+      std::vector<int64_t> cr(a1 - a0 + 1);
+      for (int64_t a = a0; a <= a1; ++a) cr[a - a0] = arow_h[a] - arow_h[a0];
+      VCK(cudaMemcpyAsync(crow.p, cr.data(), cr.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+      VCK(cudaMemsetAsync(acount.p, 0, (a1 - a0) * sizeof(int32_t), s));
+      pt2_fill(c->keys.p, n, L, pv, conn_view(c), a0, a1, crow.p, acount.p, ecol.p, eval.p, s);
+      cudaEvent_t r0, r1;
+      VCK(cudaEventCreate(&r0));
+      VCK(cudaEventCreate(&r1));
+      VCK(cudaEventRecord(r0, s));
+      pt2_en(pkeys.p, a0, a1, L, conn_view(c), crow.p, ecol.p, eval.p, c->X.p, c->ldx, nopt,
+             Ed.p, part.p, s);
+      VCK(cudaEventRecord(r1, s));
+      reduce_parts(part.p, nblk, nopt, dEd.p, s);
+      VCK(cudaEventSynchronize(r1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r0, r1);
+      cudaEventDestroy(r0);
+      cudaEventDestroy(r1);
+      c->stats.ms_pt2_reduce += ms;
+      const int64_t ent = cr.back();
+      c->stats.pt2_reduce_bytes += ent * (4 + 8) + ent * (int64_t)nopt * 8 + (a1 - a0) * (8 + 8 * L.W);
+    }
+    VCK(cudaMemcpyAsync(dE.data(), dEd.p, nopt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    VCK(cudaStreamSynchronize(s));
+    VCK(cudaGetLastError());
+    int fl = 0;
+    VTRY(read_flags(c, &fl));
+    if (fl & kFlagTableFull) return fail(c, VHCI_E_TABLE_FULL, "perturber hash full");
+    pkeys.release(s); pslots.release(s); acount.release(s); arow.release(s); tmp.release(s);
+    ecol.release(s); eval.release(s); part.release(s); dEd.release(s); Ed.release(s); crow.release(s);
+  }
+  for (int j = 0; j < nopt; ++j) {
+    c->E[j] += dE[j];
+    if (dE_out) dE_out[j] = dE[j];
+  }
+  VCK(cudaEventRecord(t1, s));
+  VCK(cudaEventSynchronize(t1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  c->stats.ms_pt2 += ms;
+  if (n_pert) *n_pert = np;
+  return VHCI_OK;
+}
+
+}  // namespace vhci
+
+using namespace vhci;
+
+namespace {
+
+void print_sparse(vhci_ctx* c) {
+  const double nn = (double)c->n;
+  const double stored = (double)(c->nnz + c->n);
+  std::cout << "The Hamiltonian is " << std::fixed << std::setprecision(2)
+            << 100 * (1. - stored / (nn * nn)) << "% sparse." << std::endl;
+}
+
+int write_cp(vhci_ctx* c, const char* path) {
+  if (!path) return VHCI_OK;
+  if (c->o.verbose) { std::cout << " Writing checkpoint file..."; std::cout.flush(); }
+  const int r = vhci_write_checkpoint(c, path);
+  if (c->o.verbose) {
+    if (r == VHCI_OK) std::cout << "done." << '\n' << std::endl;
+    else std::cout << '\n' << " Error: checkpoint file could not be found or no name was given." << '\n' << std::endl;
+  }
+  return VHCI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vhci_status vhci_hci(vhci_ctx* c, const char* checkpoint_path, vhci_iter_cb cb, void* user) {
+  if (!c) return VHCI_E_INPUT;
+  const bool v = c->o.verbose != 0;
+  const int k = c->M.nstate;
+  cudaEvent_t t0, t1;
+  VCK(cudaEventCreate(&t0));
+  VCK(cudaEventCreate(&t1));
+  VCK(cudaEventRecord(t0, c->st));
+  if (c->M.eps1 == 0.0) {  // conventional VCI over the initial basis (VHCI.cpp:49-76)
+    if (!c->restart || c->nvec == 0) {
+      if (v) { std::cout << "Constructing the Vibrational CI Hamiltonian..."; std::cout.flush(); }
+      VTRY(build_h(c));
+      if (v) {
+        print_sparse(c);
+        if (k == 1) std::cout << "done." << "\n" << "\n" << "Solving for the ground state..." << "\n" << std::endl;
+        else std::cout << "done." << "\n" << "\n" << "Solving for the lowest " << k << " eigenstates..." << "\n" << std::endl;
+      }
+      VTRY(eigs(c, k));
+      if (c->n > 100000) write_cp(c, checkpoint_path);
+    }
+  } else {  // heat-bath iterations (HB.cpp:176-265)
+    int iter = 1;
+    if (!c->restart) {
+      if (v) {
+        std::cout << " Initial basis size is: " << c->n << "\n";
+        std::cout << " Constructing Hamiltonian...";
+      }
+      VTRY(build_h(c));
+      if (v) std::cout << " Diagonalizing..." << std::endl;
+      const int guard = std::max(4, k / 10);
+      VTRY(dense_eigs(c, k + guard));
+      if (v) std::cout << std::fixed << std::setprecision(2) << " ZPE is: " << c->E[0] << "\n" << std::endl;
+      if (cb) cb(user, 0, c->n, c->E[0]);
+    }
+    for (;;) {
+      if (v) std::cout << " Performing HCI iteration: " << iter << std::endl;
+      int64_t nnew = 0;
+      VTRY(vhci_select(c, c->M.eps1, 0, &nnew));
+      if ((double)nnew / (double)c->n <= 0.01) {
+        if (v) std::cout << " Basis converged after " << iter - 1 << " iterations and contains "
+                         << c->n << " product states." << std::endl;
+        break;
+      }
+      VTRY(append_keys(c, c->sel.p, c->nsel));
+      if (v) {
+        std::cout << " Basis size after iteration " << iter << " is: " << c->n << std::endl;
+        std::cout << " Constructing Hamiltonian...";
+        std::cout.flush();
+      }
+      ++iter;
+      VTRY(build_h(c));
+      if (v) {
+        print_sparse(c);
+        if (k == 1) std::cout << " Finding the ground state..." << std::endl;
+        else std::cout << " Finding the first " << k << " eigenstates..." << std::endl;
+      }
+      VTRY(eigs(c, k));
+      c->stats.hci_iterations += 1;
+      if (v) std::cout << std::fixed << std::setprecision(2) << " ZPE is: " << c->E[0] << std::endl << std::endl;
+      if (cb) cb(user, iter - 1, c->n, c->E[0]);
+      if (c->n > 100000) write_cp(c, checkpoint_path);
+    }
+  }
+  VCK(cudaEventRecord(t1, c->st));
+  VCK(cudaEventSynchronize(t1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  c->stats.ms_total += ms;
+  return VHCI_OK;
+}
+
+vhci_status vhci_pt2(vhci_ctx* c, double eps2, double* dE, int64_t* n_pert) {
+  if (!c) return VHCI_E_INPUT;
+  const bool v = c->o.verbose != 0;
+  if (v) std::cout << " Finding connected states..." << std::endl;
+  int64_t np = 0;
+  const int r = pt2(c, eps2, dE, &np);
+  if (r != VHCI_OK) return r;
+  c->stats.ms_total += 0;
+  if (v) {
+    const int nopt = (int)std::min<int64_t>(c->M.nstate, c->n);
+    std::cout << " Perturbative space contains " << np << " states." << std::endl;
+    if (c->M.nstate == 1)
+      std::cout << " Calculating the 2nd-order perturbative correction on the ground state energy" << std::endl;
+    else
+      std::cout << " Calculating the 2nd-order perturbative correction for on first " << nopt << " eigenvalues." << std::endl;
+    std::cout << std::fixed << std::setprecision(2) << " New ZPE after PT2 correction is: " << c->E[0] << std::endl;
+  }
+  if (n_pert) *n_pert = np;
+  return VHCI_OK;
+}
+
+// PrintFreqs (Ham.cpp:448-502): line 0 = E_0 and the assignments of every basis state whose
+// |C_m0| >= max|C_0| / 2 (no separator between them); line n = E_n - E_0 with assignments
+// separated by two spaces.  min(Nstate, #eigenvalues) lines.
+vhci_status vhci_write_freqs(const vhci_ctx* c0, const char* path) {
+  vhci_ctx* c = const_cast<vhci_ctx*>(c0);
+  if (!c || !path) return VHCI_E_INPUT;
+  const int held = (int)std::min<int64_t>((int64_t)c->E.size(), c->nvec);
+  const int nf = std::min(c->M.nstate, held);
+  if (nf < 1) return fail(c, VHCI_E_STATE, "no eigenpairs to print");
+  const int64_t n = c->n;
+  const int nm = c->M.nm;
+  std::vector<uint8_t> q((size_t)n * nm);
+  int64_t nn = 0;
+  VTRY(vhci_get_basis(c, q.data(), n, &nn));
+  std::vector<double> C((size_t)n * nf);
+  VTRY(vhci_get_vectors(c, C.data(), nullptr, nf));
+  std::ofstream out(path);
+  if (!out.good()) return fail(c, VHCI_E_INPUT, "Error: Could not output file.");
+  auto assign = [&](int64_t m, std::ostream& os) {
+    int nmode = 0;
+    for (int l = 0; l < nm; ++l) {
+      const int qq = q[(size_t)m * nm + l];
+      if (qq > 0) {
+        if (nmode > 0) os << "+";
+        os << qq << "w" << l;
+        ++nmode;
+      }
+    }
+  };
+  for (int s = 0; s < nf; ++s) {
+    const double* col = C.data() + (size_t)s * n;
+    double mx = -INFINITY, mn = INFINITY;
+    for (int64_t m = 0; m < n; ++m) { mx = std::max(mx, col[m]); mn = std::min(mn, col[m]); }
+    const double maxcoeff = std::max(std::fabs(mx), std::fabs(mn));
+    if (s == 0) out << std::fixed << std::setprecision(10) << c->E[0] << "   ";
+    else out << std::fixed << std::setprecision(12) << c->E[s] - c->E[0] << "   ";
+    int state = 0;
+    for (int64_t m = 0; m < n; ++m) {
+      if (std::fabs(col[m]) >= maxcoeff / 2) {
+        if (s > 0 && state > 0) out << "  ";
+        out << std::fixed << std::setprecision(2) << std::fabs(col[m]) << " (";
+        assign(m, out);
+        out << ")";
+        ++state;
+      }
+    }
+    out << '\n';
+  }
+  out.flush();
+  return VHCI_OK;
+}
+
+// WriteCheckpoint (Core_functions.cpp:94-117): "N M NEig", then frequencies and eigenvalues,
+// then one row per basis state: quanta followed by its coefficients, all reals "%.17f".
+vhci_status vhci_write_checkpoint(const vhci_ctx* c0, const char* path) {
+  vhci_ctx* c = const_cast<vhci_ctx*>(c0);
+  if (!c || !path) return VHCI_E_INPUT;
+  if (std::string(path) == "none") return fail(c, VHCI_E_INPUT, "no checkpoint name given");
+  const int64_t n = c->n;
+  const int nm = c->M.nm;
+  const int nv = (int)std::min<int64_t>(std::min<int64_t>(c->nvec, c->M.nstate), n);
+  std::vector<uint8_t> q((size_t)n * nm);
+  int64_t nn = 0;
+  VTRY(vhci_get_basis(c, q.data(), n, &nn));
+  std::vector<double> C((size_t)n * std::max(nv, 1));
+  if (nv > 0) VTRY(vhci_get_vectors(c, C.data(), nullptr, nv));
+  FILE* f = std::fopen(path, "w");
+  if (!f) return fail(c, VHCI_E_INPUT, "checkpoint file could not be opened");
+  std::fprintf(f, "%lld %d %d\n", (long long)n, nm, c->M.nstate);
+  for (int j = 0; j < nm; ++j) std::fprintf(f, "%.17f ", c->M.freq[j]);
+  for (int j = 0; j < nv; ++j) std::fprintf(f, "%.17f ", c->E[j]);
+  std::fprintf(f, "\n");
+  for (int64_t i = 0; i < n; ++i) {
+    for (int j = 0; j < nm; ++j) std::fprintf(f, "%d ", (int)q[(size_t)i * nm + j]);
+    for (int j = 0; j < nv; ++j) std::fprintf(f, "%.17f ", C[(size_t)j * n + i]);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+  return VHCI_OK;
+}
+
+// ReadCheckpoint (Core_functions.cpp:119-167): validates the mode count, Nstate and the
+// frequencies (exact equality), then replaces the basis and the vectors.
+vhci_status vhci_read_checkpoint(vhci_ctx* c, const char* path) {
+  if (!c || !path) return VHCI_E_INPUT;
+  std::ifstream in(path);
+  if (!in.good()) return fail(c, VHCI_E_INPUT, "checkpoint file could not be opened");
+  long long nb = 0;
+  int m = 0, ne = 0;
+  in >> nb >> m >> ne;
+  if (!in || nb <= 0) return fail(c, VHCI_E_INPUT, "Error: malformed checkpoint file.");
+  if (m != c->M.nm) return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong number of fundamental modes!");
+  if (ne != c->M.nstate) return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong number of eigenstates!");
+  for (int i = 0; i < m; ++i) {
+    double f = 0;
+    in >> f;
+    if (f != c->M.freq[i]) return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong fundamental frequencies!");
+  }
+  std::vector<double> E(ne);
+  for (int i = 0; i < ne; ++i) in >> E[i];
+  std::vector<uint8_t> q((size_t)nb * m);
+  std::vector<double> C((size_t)nb * ne);
+  for (long long i = 0; i < nb; ++i) {
+    for (int j = 0; j < m; ++j) {
+      int qq = 0;
+      in >> qq;
+      if (qq < 0 || qq > 255) return fail(c, VHCI_E_KEY_OVERFLOW, "checkpoint quanta out of range");
+      q[(size_t)i * m + j] = (uint8_t)qq;
+    }
+    for (int j = 0; j < ne; ++j) in >> C[(size_t)j * nb + i];
+  }
+  if (!in) return fail(c, VHCI_E_INPUT, "Error: truncated checkpoint file.");
+  VTRY(vhci_set_basis(c, q.data(), nb));
+  VTRY(vhci_set_vectors(c, C.data(), E.data(), ne));
+  c->restart = 1;
+  return VHCI_OK;
+}
+
+}  // extern "C"

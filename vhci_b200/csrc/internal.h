@@ -1,0 +1,53 @@
+// Internal entry points shared by the host translation units of the library.
+#pragma once
+
+#include <string>
+
+#include "ctx.h"
+
+namespace vhci {
+
+int fail(vhci_ctx* c, int code, const std::string& msg);
+int cuda_fail(vhci_ctx* c, cudaError_t e, const char* where);
+int blas_fail(vhci_ctx* c, int st, const char* where);
+
+#define VCK(call)                                              \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return ::vhci::cuda_fail(c, e_, #call); \
+  } while (0)
+#define VBL(call)                                              \
+  do {                                                         \
+    int s_ = (int)(call);                                      \
+    if (s_ != 0) return ::vhci::blas_fail(c, s_, #call);       \
+  } while (0)
+#define VTRY(call)          \
+  do {                      \
+    int r_ = (call);        \
+    if (r_ != VHCI_OK) return r_; \
+  } while (0)
+
+HashView basis_view(vhci_ctx* c);
+ConnDev conn_view(vhci_ctx* c);
+HBTable hb_view(vhci_ctx* c);
+
+// Reads (and clears) the kernel flag word; returns VHCI_OK or a CUDA error.
+int read_flags(vhci_ctx* c, int* flags);
+int upload_tables(vhci_ctx* c);
+int promote_layout(vhci_ctx* c);
+int ensure_hash(vhci_ctx* c, int64_t n_total);
+int append_keys(vhci_ctx* c, const uint64_t* dkeys, int64_t m);
+
+// Heat-bath candidate set at threshold eps over the held vectors: sorted keys in c->sel,
+// count in c->nsel.  Promotes the key layout and retries when a state needs 8-bit fields.
+int generate_new_set(vhci_ctx* c, double eps);
+
+int build_h(vhci_ctx* c);
+// Lowest k eigenpairs; dense_all keeps every eigenpair of a dense solve (first HCI step).
+int eigs(vhci_ctx* c, int k);
+int dense_eigs(vhci_ctx* c, int keep);
+int pt2(vhci_ctx* c, double eps2, double* dE, int64_t* n_pert);
+
+float event_ms(vhci_ctx* c);
+
+}  // namespace vhci

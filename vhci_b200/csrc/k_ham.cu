@@ -1,0 +1,283 @@
+// Hamiltonian kernels: the connection-driven sparse build (replacing the reference's O(N^2) pair
+// loop, Ham.cpp:228-326), the SpMM that drives the eigensolver, and the Davidson vector helpers.
+#include "conn.cuh"
+#include "ops.h"
+
+namespace vhci {
+
+namespace {
+
+inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+}  // namespace
+
+namespace {
+
+// One warp per row; lanes stride over the connection groups, probe the basis hash and compact
+// the hits with a ballot, so a row's entries land in group order (deterministic layout).
+template <int W, bool FILL>
+__global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ keys, int64_t n,
+                                                KeyLayout L, HashView basis, ConnDev cd,
+                                                int32_t* __restrict__ rowcnt,
+                                                const int64_t* __restrict__ rowptr,
+                                                int32_t* __restrict__ col,
+                                                double* __restrict__ val,
+                                                float* __restrict__ valf,
+                                                double* __restrict__ diag) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += warps) {
+    uint64_t k[W];
+    load_key<W>(keys, i, k);
+    const int64_t pos = FILL ? rowptr[i] : 0;
+    int cnt = 0;
+    for (int64_t u0 = 0; u0 < cd.ngroups; u0 += 32) {
+      const int64_t u = u0 + lane;
+      int64_t j = -1;
+      GroupDev g;
+      if (u < cd.ngroups) {
+        g = cd.groups[u];
+        uint64_t t[W];
+        if (group_target<W>(cd, u, g, k, L, t)) j = hash_find<W>(basis, t, key_hash<W>(t));
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, j >= 0);
+      if (FILL && j >= 0) {
+        const int64_t p = pos + cnt + __popc(b & lanemask_lt());
+        col[p] = (int32_t)j;
+        const double v = group_value<W>(cd, g.tb, g.te, k, L);
+        if (valf) valf[p] = (float)v; else val[p] = v;
+      }
+      cnt += __popc(b);
+    }
+    if (lane == 0) {
+      if (FILL) diag[i] = diag_value<W>(cd, k, L);
+      else rowcnt[i] = cnt;
+    }
+  }
+}
+
+template <int W>
+void hbuild_count_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
+                         int32_t* rowcnt, cudaStream_t s) {
+  k_hbuild<W, false><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
+      keys, n, L, basis, cd, rowcnt, nullptr, nullptr, nullptr, nullptr, nullptr);
+}
+template <int W>
+void hbuild_fill_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
+                        const int64_t* rowptr, int32_t* col, double* val, float* valf,
+                        double* diag, cudaStream_t s) {
+  k_hbuild<W, true><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
+      keys, n, L, basis, cd, nullptr, rowptr, col, val, valf, diag);
+}
+
+// Y = (D + H_off) X for b columns.  One warp per row; lanes own columns lane + 32 r; every
+// entry's X row is a contiguous b*8-byte gather (the rows are 16-byte aligned).
+template <int NR, typename VT>
+__global__ void __launch_bounds__(256) k_spmm(int64_t n, const int64_t* __restrict__ rowptr,
+                                              const int32_t* __restrict__ col,
+                                              const VT* __restrict__ val,
+                                              const double* __restrict__ diag,
+                                              const double* __restrict__ X, int ldx, int b,
+                                              double* __restrict__ Y, int ldy) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += warps) {
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    const int64_t beg = rowptr[i], end = rowptr[i + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      int jj = 0;
+      double vv = 0.0;
+      if (e < end) { jj = __ldg(col + e); vv = (double)__ldg(val + e); }
+      const int m = (int)(end - e0 < 32 ? end - e0 : 32);
+#pragma unroll 4
+      for (int t = 0; t < m; ++t) {
+        const int j = __shfl_sync(0xffffffffu, jj, t);
+        const double v = __shfl_sync(0xffffffffu, vv, t);
+        const double* xr = X + (int64_t)j * ldx;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const int c = lane + 32 * r;
+          if (c < b) acc[r] = fma(v, __ldg(xr + c), acc[r]);
+        }
+      }
+    }
+    const double d = diag[i];
+    const double* xi = X + i * ldx;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const int c = lane + 32 * r;
+      if (c < b) Y[i * ldy + c] = fma(d, xi[c], acc[r]);
+    }
+  }
+}
+
+template <typename VT>
+void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
+                   const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
+                   cudaStream_t s) {
+  const int g = grid_for(n * 32, 256, 148 * 16);
+  switch ((b + 31) / 32) {
+#define VHCI_SPMM_CASE(R) \
+  case R: k_spmm<R, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy); break;
+    VHCI_SPMM_CASE(1) VHCI_SPMM_CASE(2) VHCI_SPMM_CASE(3) VHCI_SPMM_CASE(4)
+    VHCI_SPMM_CASE(5) VHCI_SPMM_CASE(6) VHCI_SPMM_CASE(7) VHCI_SPMM_CASE(8)
+    VHCI_SPMM_CASE(9) VHCI_SPMM_CASE(10) VHCI_SPMM_CASE(11) VHCI_SPMM_CASE(12)
+#undef VHCI_SPMM_CASE
+    default: break;
+  }
+}
+
+__global__ void k_resid_part(const double* __restrict__ X, const double* __restrict__ HX, int64_t n,
+                             int ld, int kk, const double* __restrict__ theta,
+                             double* __restrict__ part) {
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = blockIdx.x * per, hi = min(n, lo + per);
+  for (int c = threadIdx.x; c < kk; c += blockDim.x) {
+    const double th = theta[c];
+    double s = 0.0;
+    for (int64_t i = lo; i < hi; ++i) {
+      const double r = HX[i * ld + c] - th * X[i * ld + c];
+      s = fma(r, r, s);
+    }
+    part[(int64_t)blockIdx.x * kk + c] = s;
+  }
+}
+
+__global__ void k_sum_parts(const double* __restrict__ part, int nblk, int kk,
+                            double* __restrict__ out, int accumulate) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kk; c += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * kk + c];
+    out[c] = accumulate ? out[c] + s : s;
+  }
+}
+
+__global__ void k_correction(const double* __restrict__ X, const double* __restrict__ HX, int ldx,
+                             const double* __restrict__ diag, int64_t n,
+                             const int* __restrict__ cols, const double* __restrict__ theta,
+                             int nc, double* __restrict__ T, int ldt) {
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n * nc;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / nc;
+    const int j = (int)(idx % nc);
+    const int c = cols[j];
+    const double th = theta[c];
+    const double r = HX[i * ldx + c] - th * X[i * ldx + c];
+    double den = th - diag[i];
+    const double g = 1e-6 * fmax(1.0, fabs(th));
+    if (fabs(den) < g) den = den < 0 ? -g : g;
+    T[i * ldt + j] = r / den;
+  }
+}
+
+__global__ void k_copy_cols(const double* __restrict__ src, int lds, double* __restrict__ dst,
+                            int ldd, int64_t n, int ncol) {
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n * ncol;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / ncol;
+    const int c = (int)(idx % ncol);
+    dst[i * ldd + c] = src[i * lds + c];
+  }
+}
+
+template <typename VT>
+__global__ void k_dense_from_csr(int64_t n, const int64_t* __restrict__ rowptr,
+                                 const int32_t* __restrict__ col, const VT* __restrict__ val,
+                                 const double* __restrict__ diag, double* __restrict__ A) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) A[i * n + col[e]] = (double)val[e];
+    A[i * n + i] = diag[i];
+  }
+}
+
+__global__ void k_fill_zero(double* p, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = 0.0;
+}
+
+__global__ void k_set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nr) X[rows[r] * ldx + col0 + r] = 1.0;
+}
+
+}  // namespace
+
+void hbuild_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
+                  int32_t* rowcnt, cudaStream_t s) {
+  if (n <= 0) return;
+  VHCI_DISPATCH_W(L.W, hbuild_count_launch, keys, n, L, basis, cd, rowcnt, s);
+}
+
+void hbuild_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
+                 const int64_t* rowptr, int32_t* col, double* val, float* valf, double* diag,
+                 cudaStream_t s) {
+  if (n <= 0) return;
+  VHCI_DISPATCH_W(L.W, hbuild_fill_launch, keys, n, L, basis, cd, rowptr, col, val, valf, diag, s);
+}
+
+void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
+          const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
+          int ldy, cudaStream_t s) {
+  if (n <= 0 || b <= 0) return;
+  if (valf) spmm_dispatch<float>(n, rowptr, col, valf, diag, X, ldx, b, Y, ldy, s);
+  else spmm_dispatch<double>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy, s);
+}
+
+int residual_blocks(int64_t n) {
+  int64_t b = (n + 1023) / 1024;
+  if (b > 148 * 4) b = 148 * 4;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,
+                    const double* theta, double* part, int nblk, double* rn2, cudaStream_t s) {
+  k_resid_part<<<nblk, 256, 0, s>>>(X, HX, n, ld, kk, theta, part);
+  k_sum_parts<<<(kk + 255) / 256, 256, 0, s>>>(part, nblk, kk, rn2, 0);
+}
+
+void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
+                         int64_t n, const int* cols, const double* theta, int nc, double* T,
+                         int ldt, cudaStream_t s) {
+  if (nc <= 0 || n <= 0) return;
+  k_correction<<<grid_for(n * nc, 256), 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, nc, T, ldt);
+}
+
+void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,
+               cudaStream_t s) {
+  if (n <= 0 || ncol <= 0) return;
+  k_copy_cols<<<grid_for(n * ncol, 256), 256, 0, s>>>(src, lds, dst, ldd, n, ncol);
+}
+
+void dense_from_csr(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
+                    const float* valf, const double* diag, double* A, cudaStream_t s) {
+  fill_zero(A, n * n, s);
+  if (valf) k_dense_from_csr<float><<<grid_for(n, 128), 128, 0, s>>>(n, rowptr, col, valf, diag, A);
+  else k_dense_from_csr<double><<<grid_for(n, 128), 128, 0, s>>>(n, rowptr, col, val, diag, A);
+}
+
+void fill_zero(double* p, int64_t n, cudaStream_t s) {
+  if (n > 0) k_fill_zero<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+}
+
+void set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr, cudaStream_t s) {
+  if (nr > 0) k_set_unit_rows<<<(nr + 127) / 128, 128, 0, s>>>(X, ldx, col0, rows, nr);
+}
+
+void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cudaStream_t s) {
+  k_sum_parts<<<(nopt + 255) / 256, 256, 0, s>>>(part, nblk, nopt, out_accum, 1);
+}
+
+}  // namespace vhci

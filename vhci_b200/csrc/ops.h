@@ -1,0 +1,139 @@
+// Host launchers for the device kernels.  All launches are asynchronous on the given stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace vhci {
+
+// ---- device table records ----
+struct GroupDev {   // one connection group (a fixed quanta change)
+  int32_t tb, te;   // term range
+  uint8_t nchg;
+  uint8_t mode[6];
+  int8_t delta[6];
+  uint8_t pad[3];
+};
+struct TermDev {    // one FC term of a group: fc * prod_j T[pw_j][q(mode_j)][dl_j]
+  double fc;
+  uint8_t nk;
+  uint8_t mode[6];
+  uint8_t pw[6];
+  int8_t dl[6];
+  uint8_t pad[5];
+};
+struct HBDev {      // heat-bath list entry (pattern decoder)
+  int32_t zero_idx;
+  uint8_t nk;
+  uint8_t mode[6];
+  uint8_t pw[6];
+  uint8_t pad[3];
+};
+static_assert(sizeof(GroupDev) == 24, "GroupDev layout");
+static_assert(sizeof(TermDev) == 32, "TermDev layout");
+static_assert(sizeof(HBDev) == 20, "HBDev layout");
+
+struct ConnDev {            // connection tables on device
+  const GroupDev* groups;
+  const int64_t* wdelta;    // [ngroups * W] packed key change per word
+  int64_t ngroups;
+  const TermDev* terms;
+  const TermDev* dterms;    // Delta = 0 terms
+  int ndterms;
+  const double* T;          // ladder table, (qmax+1) stride
+  const double* freq;       // [nm]
+  int nm;
+};
+
+struct HBTable {
+  const HBDev* e;
+  const double* absfc;      // [nhb] |fc| descending
+  const int64_t* cum;       // [nhb+1] exclusive prefix of pattern counts
+  int nhb;
+};
+
+// ---- scan / utilities (k_basis.cu) ----
+// Exclusive prefix sum of n int64 values into out (may alias in); returns nothing, total is
+// written to out[n] (out must hold n+1).  tmp must hold scan_tmp_elems(n) int64.
+int64_t scan_tmp_elems(int64_t n);
+void exclusive_scan(const int64_t* in, int64_t* out, int64_t n, int64_t* tmp, cudaStream_t s);
+void exclusive_scan_i32(const int32_t* in, int64_t* out, int64_t n, int64_t* tmp, cudaStream_t s);
+
+// ---- keys and hash ----
+void pack_keys(const uint8_t* quanta, int64_t n, int nm, KeyLayout L, uint64_t* keys,
+               cudaStream_t s);
+void unpack_keys(const uint64_t* keys, int64_t n, int nm, KeyLayout L, uint8_t* quanta,
+                 cudaStream_t s);
+void repack_keys(const uint64_t* in, KeyLayout from, uint64_t* out, KeyLayout to, int64_t n,
+                 int nm, cudaStream_t s);
+void hash_clear(uint64_t* slots, uint64_t nslots, cudaStream_t s);
+void hash_insert_range(uint64_t* slots, uint64_t mask, const uint64_t* keys, int64_t begin,
+                       int64_t end, int W, int* flags, cudaStream_t s);
+void max_quanta_per_mode(const uint64_t* keys, int64_t n, int nm, KeyLayout L, int* out,
+                         cudaStream_t s);
+
+// ---- heat-bath selection ----
+// cmax[i] = signed C_ij of max |C_ij| over j < nopt (first occurrence); X row-major, ld = ldx.
+void cmax_rows(const double* X, int64_t n, int ldx, int nopt, double* cmax, cudaStream_t s);
+// work[i] = number of patterns generated by state i at threshold eps.
+void select_count(const double* cmax, int64_t n, HBTable hb, double eps, int64_t* work,
+                  cudaStream_t s);
+// Generate candidates for work items [0, total): probe the basis hash, insert absent keys into
+// the new-state set.
+void select_generate(const uint64_t* keys, int64_t n, const int64_t* woff, int64_t total,
+                     HBTable hb, KeyLayout L, HashView basis, NewSetView ns, cudaStream_t s);
+// Compact live candidates into out (count written to *n_out on device).
+void newset_compact(const uint64_t* cand, const uint8_t* dead, int64_t ncand, int W,
+                    uint64_t* out, unsigned long long* n_out, cudaStream_t s);
+
+// ---- radix sort of packed keys (ascending, most significant word last) ----
+// Sorts n keys of W words in place using `alt` (n*W words) as the ping-pong buffer; only the low
+// `nbits` bits of the key (mode fields in use) are examined.  hist must hold
+// radix_hist_elems(n) int64.
+int64_t radix_hist_elems(int64_t n);
+void radix_sort_keys(uint64_t* keys, uint64_t* alt, int64_t n, int W, int nbits, int64_t* hist,
+                     cudaStream_t s);
+
+// ---- Hamiltonian (k_ham.cu) ----
+void hbuild_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
+                  int32_t* rowcnt, cudaStream_t s);
+void hbuild_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
+                 const int64_t* rowptr, int32_t* col, double* val, float* valf, double* diag,
+                 cudaStream_t s);
+// Y[:, 0:b] = H X[:, 0:b] with H = diag + off-diagonal CSR (FP64 or FP32 values).
+void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
+          const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
+          int ldy, cudaStream_t s);
+// ---- Davidson helpers ----
+// rn2[c] (c < kk) = sum_i (HX[i,c] - theta[c] X[i,c])^2   (block partials reduced on device)
+void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,
+                    const double* theta, double* part, int nblk, double* rn2, cudaStream_t s);
+int residual_blocks(int64_t n);
+// T[i, j] = (HX[i,c_j] - theta_j X[i,c_j]) / (theta_j - d_i), c_j = cols[j]
+void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
+                         int64_t n, const int* cols, const double* theta, int nc, double* T,
+                         int ldt, cudaStream_t s);
+void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,
+               cudaStream_t s);
+void dense_from_csr(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
+                    const float* valf, const double* diag, double* A, cudaStream_t s);
+void fill_zero(double* p, int64_t n, cudaStream_t s);
+void set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr, cudaStream_t s);
+
+// ---- PT2 (k_pt2.cu) ----
+void pt2_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
+               int64_t a_lo, int64_t a_hi, int32_t* acount, cudaStream_t s);
+void pt2_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
+              int64_t a_lo, int64_t a_hi, const int64_t* arowptr, int32_t* afill, int32_t* ecol,
+              double* eval, cudaStream_t s);
+// Fused EN reduction over perturbers [a_lo, a_hi): num_a = sum_e eval_e X[ecol_e, :nopt];
+// E_a = harmonic + diagonal terms; part[blk][n] += num^2 / (E_n - E_a).
+int pt2_en_blocks();
+void pt2_en(const uint64_t* pkeys, int64_t a_lo, int64_t a_hi, KeyLayout L, ConnDev cd,
+            const int64_t* arowptr, const int32_t* ecol, const double* eval, const double* X,
+            int ldx, int nopt, const double* E, double* part, cudaStream_t s);
+void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cudaStream_t s);
+
+}  // namespace vhci
