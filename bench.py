@@ -1,0 +1,324 @@
+"""Benchmark: heat-bath VCI + Epstein-Nesbet PT2 solve of the workload-1 synthetic PES.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision 0|1]
+
+Workload (one "step" = one full solve): seeded synthetic PES with Nm = 15 modes (cubic keep
+p = 0.5, values +-10^U(0,2.5); quartic keep p = 0.3, values +-10^U(-1,1.5), diagonal positive),
+HCI_Eps = 0.5, Nstate = 200, PT2 on with PT2_Eps = 0.01, Max_quanta = 2.  The solve runs the
+reference procedure: dense first step, heat-bath iterations with a sparse eigensolve each, then
+PT2 over the screened perturber space.
+
+Our arm (default): the library (libvhci_gpu.so, sm_100a) through its C ABI.
+  value  = seconds per solve over the whole job (max over ranks of the timed region, divided by the
+           solves all ranks completed), device-timed with CUDA events on the library's stream with
+           the problem tables resident on the device;
+  e2e    = the same through the public call a user makes (`vhci_b200.solve(path)`: parse, upload,
+           solve, read the energies back), wall-clocked around synchronised steps.
+  N > 1 GPUs run independent replicas (requests do not share data): weak scaling, no collective
+  on the data path; ranks meet only at the timing barriers.
+Reference arm (--impl reference): the reference algorithm on the host cores, as the CPU oracle's
+literal restatement of its pair loop (src/Ham.cpp:237-323, the same body as src/PT2.cpp:70-118),
+timed on a bounded sample of rows and extrapolated to the workload's pair count (the basis sizes
+per iteration and |P| below, which any implementation of the algorithm reproduces).  Selection
+and eigensolver time are not added, so it is a lower bound on the reference's time per solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = 1
+WORKLOAD_DESC = ("VHCI+PT2, synthetic PES Nm=15 (cubic p=0.5 +-10^U(0,2.5), quartic p=0.3 "
+                 "+-10^U(-1,1.5)), HCI_Eps=0.5, Nstate=200, PT2_Eps=0.01, Max_quanta=2")
+# Basis size after each heat-bath iteration and |P| of the workload-1 solve (FP64 path).
+WORKLOAD_COUNTS = {"sizes": [38934, 215006, 336950, 372333, 380418], "n_pert": 6583465}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names[1:], p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def write_workload(path: str) -> None:
+    from vhci_b200 import pes
+    pes.write_config(path, WORKLOAD)
+
+
+# ------------------------------------------------------------------------------ reference arm
+
+def reference_sample(budget_s: float = 15.0) -> dict:
+    """Time the reference pair loop on rows of the workload's first-iteration basis with all host
+    threads; return seconds per solve extrapolated to the workload's pair count."""
+    import numpy as np
+    from oracle import oracle as O
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "workload.inp")
+        write_workload(path)
+        o = O.Oracle(path)
+        w, C = np.linalg.eigh(o.dense_h())
+        o.append_basis(o.select(C, min(o.neig, o.n), o.eps1))
+        n = o.n
+        threads = int(O.lib().orc_num_threads())
+        # grow the row sample until it takes about budget_s
+        stride = max(1, n // 64)
+        pairs, dt = 0, 0.0
+        while True:
+            t0 = time.perf_counter()
+            p, _ = O.pair_rows(o, 0, n, stride)
+            d = time.perf_counter() - t0
+            pairs += p
+            dt += d
+            if dt >= budget_s or stride == 1:
+                break
+            stride = max(1, int(stride * d / max(budget_s - dt, 1e-3) / 2) or 1)
+    per_pair = dt / pairs
+    sizes, npert = WORKLOAD_COUNTS["sizes"], WORKLOAD_COUNTS["n_pert"]
+    total_pairs = sum(s * (s + 1) / 2 for s in sizes) + npert * sizes[-1]
+    return {"s_per_solve": per_pair * total_pairs, "threads": threads, "pairs_timed": pairs,
+            "seconds_timed": dt, "sample_basis": n, "ns_per_pair": per_pair * 1e9,
+            "total_pairs": total_pairs}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = reference_sample(args.ref_budget)
+        if i >= args.warmup:
+            vals.append(info["s_per_solve"])
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "s/solve", "value": v, "unit": "s/solve",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC, "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "s/solve", "cores": info["threads"], "kind": "port",
+                         "sample": (f"literal reference pair loop, {info['pairs_timed']:.3g} pairs on "
+                                    f"the first-iteration basis ({info['sample_basis']} states) in "
+                                    f"{info['seconds_timed']:.1f} s, extrapolated to "
+                                    f"{info['total_pairs']:.3g} pairs (H builds + PT2); "
+                                    "selection and eigensolver time not included")},
+        "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------ our arm
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from vhci_b200 import api
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    td = tempfile.mkdtemp(prefix="vhci_bench_")
+    path = os.path.join(td, "workload.inp")
+    write_workload(path)
+
+    ctx = api.VHCI(path, device=local, precision=args.precision)
+    q0 = ctx.basis()
+
+    def solve_resident():
+        ctx.set_basis(q0)
+        s0 = ctx.stats()
+        ctx.hci()
+        ctx.pt2()
+        s1 = ctx.stats()
+        return (s1["ms_total"] - s0["ms_total"]) + (s1["ms_pt2"] - s0["ms_pt2"])
+
+    for _ in range(args.warmup):
+        solve_resident()
+    ctx.reset_stats()
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    l0 = ctx.stats()["kernel_launches"]
+    t0 = time.perf_counter()
+    dev_ms = [solve_resident() for _ in range(args.steps)]
+    barrier()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    st = ctx.stats()
+    launches = st["kernel_launches"] - l0
+    info = ctx.info
+    E = ctx.energies()
+    ctx.close()
+
+    dev_s = allmax(sum(dev_ms) / 1e3)
+    wall_s = allmax(wall)
+    value = dev_s / (args.steps * ws)
+
+    # end to end through the public call, host inputs and outputs
+    barrier()
+    e2e_t, h2d, d2h = 0.0, 0, 0
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        r = api.solve(path, device=local, precision=args.precision)
+        torch.cuda.synchronize()
+        e2e_t += time.perf_counter() - t1
+        h2d += r["stats"]["h2d_bytes"]
+        d2h += r["stats"]["d2h_bytes"]
+    barrier()
+    e2e_s = allmax(e2e_t) / (args.steps * ws)
+
+    hbm, peak_kind = measured_peaks()
+    spmm_gbs = st["spmm_bytes"] / (st["ms_spmm"] / 1e3) / 1e9 if st["ms_spmm"] else None
+    en_gbs = (st["pt2_reduce_bytes"] / (st["ms_pt2_reduce"] / 1e3) / 1e9
+              if st["ms_pt2_reduce"] else None)
+    roof = {"bound": "hbm", "kernel": "k_spmm (eigensolver H*X)", "achieved": spmm_gbs,
+            "peak": hbm, "unit": "GB/s", "frac": (spmm_gbs / hbm) if spmm_gbs else None,
+            "traffic": args.traffic, "peak_kind": peak_kind,
+            "other": {"k_pt2_en GB/s": en_gbs}}
+
+    line = {
+        "metric": "s/solve", "value": value, "unit": "s/solve", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps,
+        "wall_s_timed": wall_s, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f32-storage/f64-accum",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC, "n_basis": int(info.n_basis),
+                   "n_pert": WORKLOAD_COUNTS["n_pert"], "global_batch": ws,
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "working set larger than L2 (Hamiltonian ~2 GB), no flush needed",
+                   "E0": float(E[0])},
+        "clocks": clk,
+        "e2e": {"value": e2e_s, "unit": "s/solve", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "phase_ms": {k: round(st[k] / args.steps, 2) for k in
+                     ("ms_select", "ms_hbuild", "ms_eigs", "ms_spmm", "ms_pt2", "ms_pt2_reduce")},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ref = reference_sample(args.ref_budget)
+        line["cpu_baseline"] = {
+            "value": ref["s_per_solve"], "unit": "s/solve", "cores": ref["threads"],
+            "kind": "port",
+            "sample": (f"literal reference pair loop, {ref['pairs_timed']:.3g} pairs in "
+                       f"{ref['seconds_timed']:.1f} s, extrapolated to {ref['total_pairs']:.3g} "
+                       "pairs (H builds + PT2); selection and eigensolver time not included")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--ref-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu dram bytes per SpMM launch, if captured")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -96,6 +96,8 @@ typedef struct {
   int64_t pt2_reduce_bytes;       /* algorithmic bytes of the EN reduction                     */
   int eig_iterations;             /* Davidson iterations summed over all eigensolves           */
   int hci_iterations;
+  int64_t h2d_bytes, d2h_bytes;   /* host<->device bytes copied by the library                 */
+  int64_t kernel_launches;        /* this library's kernel launches so far (process-wide)      */
 } vhci_stats;
 
 typedef void (*vhci_iter_cb)(void* user, int iteration, int64_t n_basis, double zpe);

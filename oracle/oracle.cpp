@@ -663,6 +663,30 @@ int64_t orc_pt2(void* p, const double* C, int ncols, const double* E, int nopt, 
   return np;
 }
 
+// Timed sample of the reference's pair loop (src/Ham.cpp:237-323, the same body as
+// src/PT2.cpp:70-118): rows i = r0, r0+stride, ... < r1, each against every j >= i, in parallel
+// over rows.  Returns the number of (i, j) pairs evaluated; *checksum receives the sum of values.
+int64_t orc_pair_rows(void* p, int64_t r0, int64_t r1, int64_t stride, double* checksum) {
+  Ctx& c = ((Handle*)p)->c;
+  const int64_t n = (int64_t)c.basis.size();
+  int64_t pairs = 0;
+  double sum = 0.0;
+#pragma omp parallel reduction(+ : pairs, sum)
+  {
+    std::vector<int> d(c.nm);
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t i = r0; i < r1; i += stride) {
+      for (int64_t j = i; j < n; ++j) {
+        double v;
+        if (pair_value(c, c.basis[i], c.basis[j], d, v)) sum += v;
+      }
+      pairs += n - i;
+    }
+  }
+  if (checksum) *checksum = sum;
+  return pairs;
+}
+
 // Ladder factor <n+delta| (a + a^dag)^p |n> by the reference's path expansion (src/Ham.cpp:38-104).
 double orc_ladder(int p, int n, int delta) {
   FC f; f.fc = 1.0; f.fcpow.assign(p, 0); f.modes = {0}; f.powers = {p};

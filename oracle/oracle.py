@@ -67,6 +67,8 @@ def lib():
         L.orc_pt2.restype = i64
         L.orc_pt2.argtypes = [vp, dp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                               dp]
+        L.orc_pair_rows.restype = i64
+        L.orc_pair_rows.argtypes = [vp, i64, i64, i64, dp]
         L.orc_ladder.restype = ctypes.c_double
         L.orc_ladder.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_num_threads.restype = ctypes.c_int
@@ -170,6 +172,14 @@ class Oracle:
         q = np.zeros((npert, self.nm), np.int32)
         lib().orc_get_selected(self.h, _p(q, ctypes.c_int32))
         return dE, q
+
+
+def pair_rows(o: "Oracle", r0: int, r1: int, stride: int):
+    """Reference pair loop over rows r0, r0+stride, ... < r1 against all j >= i; returns
+    (pairs evaluated, checksum)."""
+    cs = ctypes.c_double()
+    n = lib().orc_pair_rows(o.h, r0, r1, stride, ctypes.byref(cs))
+    return int(n), cs.value
 
 
 def ladder(p: int, n: int, delta: int) -> float:

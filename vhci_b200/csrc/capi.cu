@@ -52,7 +52,7 @@ float event_ms(vhci_ctx* c) {
 
 int read_flags(vhci_ctx* c, int* flags) {
   int h = 0;
-  VCK(cudaMemcpyAsync(&h, c->flags.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  VCK(d2h(c, &h, c->flags.p, sizeof(int)));
   VCK(cudaMemsetAsync(c->flags.p, 0, sizeof(int), c->st));
   VCK(cudaStreamSynchronize(c->st));
   *flags = h;
@@ -72,7 +72,7 @@ template <class T>
 static int upload(vhci_ctx* c, DBuf<T>& b, const std::vector<T>& h) {
   VCK(b.reserve(std::max<size_t>(h.size(), 1), c->st));
   if (!h.empty())
-    VCK(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->st));
+    VCK(h2d(c, b.p, h.data(), h.size() * sizeof(T)));
   return VHCI_OK;
 }
 
@@ -209,7 +209,7 @@ int generate_new_set(vhci_ctx* c, double eps) {
     select_count(c->d64a.p, n, hb_view(c), eps, c->i64a.p, c->st);
     exclusive_scan(c->i64a.p, c->i64a.p, n, c->scan_tmp.p, c->st);
     int64_t total = 0;
-    VCK(cudaMemcpyAsync(&total, c->i64a.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+    VCK(d2h(c, &total, c->i64a.p + n, sizeof(int64_t)));
     VCK(cudaStreamSynchronize(c->st));
     c->stats.select_candidates += total;
     c->nsel = 0;
@@ -243,13 +243,13 @@ int generate_new_set(vhci_ctx* c, double eps) {
         continue;
       }
       unsigned long long ncand = 0;
-      VCK(cudaMemcpyAsync(&ncand, c->ull.p, sizeof(ncand), cudaMemcpyDeviceToHost, c->st));
+      VCK(d2h(c, &ncand, c->ull.p, sizeof(ncand)));
       VCK(cudaStreamSynchronize(c->st));
       ncand = std::min<unsigned long long>(ncand, (unsigned long long)cap);
       VCK(c->sel.reserve((size_t)std::max<unsigned long long>(ncand, 1) * W, c->st));
       newset_compact(c->u64a.p, c->u8a.p, (int64_t)ncand, W, c->sel.p, c->ull.p + 1, c->st);
       unsigned long long m = 0;
-      VCK(cudaMemcpyAsync(&m, c->ull.p + 1, sizeof(m), cudaMemcpyDeviceToHost, c->st));
+      VCK(d2h(c, &m, c->ull.p + 1, sizeof(m)));
       VCK(cudaStreamSynchronize(c->st));
       c->nsel = (int64_t)m;
       if (m > 1) {
@@ -276,7 +276,7 @@ int build_h(vhci_ctx* c) {
   hbuild_count(c->keys.p, n, c->L, basis_view(c), conn_view(c), c->rowcnt.p, c->st);
   exclusive_scan_i32(c->rowcnt.p, c->rowptr.p, n, c->scan_tmp.p, c->st);
   int64_t nnz = 0;
-  VCK(cudaMemcpyAsync(&nnz, c->rowptr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+  VCK(d2h(c, &nnz, c->rowptr.p + n, sizeof(int64_t)));
   VCK(cudaStreamSynchronize(c->st));
   VCK(c->col.reserve(std::max<int64_t>(nnz, 1), c->st));
   if (c->o.precision == 1) {
@@ -335,7 +335,7 @@ static int create_common(vhci_ctx* c, int restart) {
   const int64_t n0 = c->M.n0;
   DBuf<uint8_t> q;
   VCK(q.reserve(std::max<int64_t>(n0 * c->M.nm, 1), c->st));
-  VCK(cudaMemcpyAsync(q.p, c->M.init_basis.data(), n0 * c->M.nm, cudaMemcpyHostToDevice, c->st));
+  VCK(h2d(c, q.p, c->M.init_basis.data(), n0 * c->M.nm));
   VCK(c->keys.reserve((size_t)std::max<int64_t>(n0, 16) * c->L.W, c->st));
   pack_keys(q.p, n0, c->M.nm, c->L, c->keys.p, c->st);
   q.release(c->st);
@@ -447,6 +447,7 @@ vhci_status vhci_get_info(const vhci_ctx* c, vhci_info* info) {
 vhci_status vhci_get_stats(const vhci_ctx* c, vhci_stats* s) {
   if (!c || !s) return VHCI_E_INPUT;
   *s = c->stats;
+  s->kernel_launches = launch_count();
   return VHCI_OK;
 }
 
@@ -494,7 +495,7 @@ vhci_status vhci_set_basis(vhci_ctx* c, const uint8_t* quanta, int64_t n) {
   }
   DBuf<uint8_t> q;
   VCK(q.reserve(n * c->M.nm, c->st));
-  VCK(cudaMemcpyAsync(q.p, quanta, n * c->M.nm, cudaMemcpyHostToDevice, c->st));
+  VCK(h2d(c, q.p, quanta, n * c->M.nm));
   VCK(c->keys.reserve((size_t)n * c->L.W, c->st));
   pack_keys(q.p, n, c->M.nm, c->L, c->keys.p, c->st);
   q.release(c->st);
@@ -520,7 +521,7 @@ vhci_status vhci_get_basis(const vhci_ctx* c0, uint8_t* quanta, int64_t cap, int
   DBuf<uint8_t> q;
   VCK(q.reserve(std::max<int64_t>(c->n * c->M.nm, 1), c->st));
   unpack_keys(c->keys.p, c->n, c->M.nm, c->L, q.p, c->st);
-  VCK(cudaMemcpyAsync(quanta, q.p, c->n * c->M.nm, cudaMemcpyDeviceToHost, c->st));
+  VCK(d2h(c, quanta, q.p, c->n * c->M.nm));
   q.release(c->st);
   VCK(cudaStreamSynchronize(c->st));
   return VHCI_OK;
@@ -533,7 +534,7 @@ vhci_status vhci_set_vectors(vhci_ctx* c, const double* C, const double* E, int 
   for (int64_t i = 0; i < n; ++i)
     for (int j = 0; j < k; ++j) h[(size_t)i * k + j] = C[(size_t)j * n + i];
   VCK(c->X.reserve((size_t)n * k, c->st));
-  VCK(cudaMemcpyAsync(c->X.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  VCK(h2d(c, c->X.p, h.data(), h.size() * sizeof(double)));
   VCK(cudaStreamSynchronize(c->st));
   c->ldx = k;
   c->nvec = k;
@@ -549,7 +550,7 @@ vhci_status vhci_get_vectors(const vhci_ctx* c0, double* C, double* E, int k) {
   const int64_t n = c->n;
   if (C) {
     std::vector<double> h((size_t)n * c->ldx);
-    VCK(cudaMemcpyAsync(h.data(), c->X.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    VCK(d2h(c, h.data(), c->X.p, h.size() * sizeof(double)));
     VCK(cudaStreamSynchronize(c->st));
     for (int64_t i = 0; i < n; ++i)
       for (int j = 0; j < k; ++j) C[(size_t)j * n + i] = h[(size_t)i * c->ldx + j];
@@ -595,7 +596,7 @@ vhci_status vhci_get_selected(const vhci_ctx* c0, uint8_t* quanta, int64_t cap, 
   DBuf<uint8_t> q;
   VCK(q.reserve(c->nsel * c->M.nm, c->st));
   unpack_keys(c->sel.p, c->nsel, c->M.nm, c->L, q.p, c->st);
-  VCK(cudaMemcpyAsync(quanta, q.p, c->nsel * c->M.nm, cudaMemcpyDeviceToHost, c->st));
+  VCK(d2h(c, quanta, q.p, c->nsel * c->M.nm));
   q.release(c->st);
   VCK(cudaStreamSynchronize(c->st));
   return VHCI_OK;
@@ -616,19 +617,19 @@ vhci_status vhci_get_h_csr(const vhci_ctx* c0, int64_t* rowptr, int32_t* col, do
   std::vector<int64_t> rp(n + 1);
   std::vector<int32_t> cl(c->nnz);
   std::vector<double> vl(c->nnz), dg(n);
-  VCK(cudaMemcpyAsync(rp.data(), c->rowptr.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, c->st));
+  VCK(d2h(c, rp.data(), c->rowptr.p, (n + 1) * sizeof(int64_t)));
   if (c->nnz) {
-    VCK(cudaMemcpyAsync(cl.data(), c->col.p, c->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, c->st));
+    VCK(d2h(c, cl.data(), c->col.p, c->nnz * sizeof(int32_t)));
     if (c->o.precision == 1) {
       std::vector<float> vf(c->nnz);
-      VCK(cudaMemcpyAsync(vf.data(), c->valf.p, c->nnz * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+      VCK(d2h(c, vf.data(), c->valf.p, c->nnz * sizeof(float)));
       VCK(cudaStreamSynchronize(c->st));
       for (int64_t e = 0; e < c->nnz; ++e) vl[e] = vf[e];
     } else {
-      VCK(cudaMemcpyAsync(vl.data(), c->val.p, c->nnz * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      VCK(d2h(c, vl.data(), c->val.p, c->nnz * sizeof(double)));
     }
   }
-  VCK(cudaMemcpyAsync(dg.data(), c->diag.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  VCK(d2h(c, dg.data(), c->diag.p, n * sizeof(double)));
   VCK(cudaStreamSynchronize(c->st));
   int64_t pos = 0;
   std::vector<std::pair<int32_t, double>> row;

@@ -8,6 +8,8 @@ namespace vhci {
 
 // Sum of a group's terms for ket key k: each term is fc * prod_j T[pw_j][q(mode_j)][dl_j], multiplied
 // left to right and summed in table order (the reference's AnharmPot product and Vij sum order).
+// Products and sums use explicit round-to-nearest operations so no multiply-add is contracted:
+// the results are the same bits as the reference's separate multiplies and adds.
 template <int W>
 __device__ __forceinline__ double group_value(const ConnDev& cd, int tb, int te,
                                               const uint64_t (&k)[W], const KeyLayout& L) {
@@ -18,9 +20,9 @@ __device__ __forceinline__ double group_value(const ConnDev& cd, int tb, int te,
     double tv = tm.fc;
     for (int j = 0; j < tm.nk; ++j) {
       const int q = key_q<W>(k, tm.mode[j], L.mpw, L.bits);
-      tv *= __ldg(cd.T + ((int64_t)tm.pw[j] * qs + q) * 13 + tm.dl[j] + 6);
+      tv = __dmul_rn(tv, __ldg(cd.T + ((int64_t)tm.pw[j] * qs + q) * 13 + tm.dl[j] + 6));
     }
-    v += tv;
+    v = __dadd_rn(v, tv);
   }
   return v;
 }
@@ -33,9 +35,9 @@ __device__ __forceinline__ double diag_value(const ConnDev& cd, const uint64_t (
   double e = 0.0;
   for (int m = 0; m < cd.nm; ++m) {
     double ej = 0.5;
-    ej += (double)key_q<W>(k, m, L.mpw, L.bits);
-    ej *= __ldg(cd.freq + m);
-    e += ej;
+    ej = __dadd_rn(ej, (double)key_q<W>(k, m, L.mpw, L.bits));
+    ej = __dmul_rn(ej, __ldg(cd.freq + m));
+    e = __dadd_rn(e, ej);
   }
   const int qs = L.qmax + 1;
   double v = 0.0;
@@ -44,11 +46,11 @@ __device__ __forceinline__ double diag_value(const ConnDev& cd, const uint64_t (
     double tv = tm.fc;
     for (int j = 0; j < tm.nk; ++j) {
       const int q = key_q<W>(k, tm.mode[j], L.mpw, L.bits);
-      tv *= __ldg(cd.T + ((int64_t)tm.pw[j] * qs + q) * 13 + 6);
+      tv = __dmul_rn(tv, __ldg(cd.T + ((int64_t)tm.pw[j] * qs + q) * 13 + 6));
     }
-    v += tv;
+    v = __dadd_rn(v, tv);
   }
-  return e + v;
+  return __dadd_rn(e, v);
 }
 
 // Target of group u from key k, or false when a changed mode leaves [0, qmax] (such a state

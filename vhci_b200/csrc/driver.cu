@@ -50,7 +50,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     pt2_count(c->keys.p, n, L, pv, conn_view(c), 0, np, acount.p, s);
     exclusive_scan_i32(acount.p, arow.p, np, tmp.p, s);
     std::vector<int64_t> arow_h(np + 1);
-    VCK(cudaMemcpyAsync(arow_h.data(), arow.p, (np + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    VCK(d2h(c, arow_h.data(), arow.p, (np + 1) * sizeof(int64_t)));
     VCK(cudaStreamSynchronize(s));
     const int64_t total = arow_h[np];
     c->stats.pt2_entries += total;
@@ -82,14 +82,14 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     VCK(dEd.reserve(nopt, s));
     VCK(Ed.reserve(nopt, s));
     VCK(cudaMemsetAsync(dEd.p, 0, nopt * sizeof(double), s));
-    VCK(cudaMemcpyAsync(Ed.p, c->E.data(), nopt * sizeof(double), cudaMemcpyHostToDevice, s));
+    VCK(h2d(c, Ed.p, c->E.data(), nopt * sizeof(double)));
     DBuf<int64_t> crow;
     for (size_t q = 1; q < bounds.size(); ++q) {
       const int64_t a0 = bounds[q - 1], a1 = bounds[q];
       VCK(crow.reserve(a1 - a0 + 1, s));
       std::vector<int64_t> cr(a1 - a0 + 1);
       for (int64_t a = a0; a <= a1; ++a) cr[a - a0] = arow_h[a] - arow_h[a0];
-      VCK(cudaMemcpyAsync(crow.p, cr.data(), cr.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+      VCK(h2d(c, crow.p, cr.data(), cr.size() * sizeof(int64_t)));
       VCK(cudaMemsetAsync(acount.p, 0, (a1 - a0) * sizeof(int32_t), s));
       pt2_fill(c->keys.p, n, L, pv, conn_view(c), a0, a1, crow.p, acount.p, ecol.p, eval.p, s);
       cudaEvent_t r0, r1;
@@ -109,7 +109,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       const int64_t ent = cr.back();
       c->stats.pt2_reduce_bytes += ent * (4 + 8) + ent * (int64_t)nopt * 8 + (a1 - a0) * (8 + 8 * L.W);
     }
-    VCK(cudaMemcpyAsync(dE.data(), dEd.p, nopt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    VCK(d2h(c, dE.data(), dEd.p, nopt * sizeof(double)));
     VCK(cudaStreamSynchronize(s));
     VCK(cudaGetLastError());
     int fl = 0;

@@ -50,4 +50,14 @@ int pt2(vhci_ctx* c, double eps2, double* dE, int64_t* n_pert);
 
 float event_ms(vhci_ctx* c);
 
+// Host<->device copies on the context stream, counted in the statistics.
+inline cudaError_t h2d(vhci_ctx* c, void* dst, const void* src, size_t bytes) {
+  c->stats.h2d_bytes += (int64_t)bytes;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st);
+}
+inline cudaError_t d2h(vhci_ctx* c, void* dst, const void* src, size_t bytes) {
+  c->stats.d2h_bytes += (int64_t)bytes;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st);
+}
+
 }  // namespace vhci

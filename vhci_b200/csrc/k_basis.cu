@@ -1,9 +1,15 @@
 // Basis-state kernels: prefix scans, key packing, the basis hash, Cmax, heat-bath candidate
 // generation with warp-free load balancing, candidate compaction and an LSD radix sort of packed
 // keys.  All are memory-bound integer/byte kernels sized in grid-stride loops.
+#include <atomic>
+
 #include "ops.h"
 
 namespace vhci {
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 namespace {
 
@@ -97,13 +103,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile(const TI* __restrict
 template <typename TI>
 void scan_impl(const TI* in, int64_t* out, int64_t n, int64_t* tmp, cudaStream_t s) {
   if (n <= kScanTile) {
-    k_scan_tile<TI><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr);
+    note_launch(); k_scan_tile<TI><<<1, kScanThreads, 0, s>>>(in, out, n, nullptr);
     return;
   }
   const int64_t nb = (n + kScanTile - 1) / kScanTile;
-  k_scan_reduce<TI><<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, tmp);
+  note_launch(); k_scan_reduce<TI><<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, tmp);
   scan_impl<int64_t>(tmp, tmp, nb, tmp + nb + 1, s);
-  k_scan_tile<TI><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, tmp);
+  note_launch(); k_scan_tile<TI><<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, tmp);
 }
 
 }  // namespace
@@ -190,7 +196,7 @@ template <int W>
 void hash_insert_launch(uint64_t* slots, uint64_t mask, const uint64_t* keys, int64_t begin,
                         int64_t end, int* flags, cudaStream_t s) {
   if (end <= begin) return;
-  k_hash_insert<W><<<grid_for(end - begin, 256), 256, 0, s>>>(slots, mask, keys, begin, end,
+  note_launch(); k_hash_insert<W><<<grid_for(end - begin, 256), 256, 0, s>>>(slots, mask, keys, begin, end,
                                                                flags);
 }
 
@@ -213,18 +219,18 @@ __global__ void k_max_quanta(const uint64_t* __restrict__ keys, int64_t n, int n
 }  // namespace
 
 void pack_keys(const uint8_t* q, int64_t n, int nm, KeyLayout L, uint64_t* keys, cudaStream_t s) {
-  if (n > 0) k_pack<<<grid_for(n, 256), 256, 0, s>>>(q, n, nm, L, keys);
+  if (n > 0) { note_launch(); k_pack<<<grid_for(n, 256), 256, 0, s>>>(q, n, nm, L, keys); }
 }
 void unpack_keys(const uint64_t* keys, int64_t n, int nm, KeyLayout L, uint8_t* q,
                  cudaStream_t s) {
-  if (n > 0) k_unpack<<<grid_for(n, 256), 256, 0, s>>>(keys, n, nm, L, q);
+  if (n > 0) { note_launch(); k_unpack<<<grid_for(n, 256), 256, 0, s>>>(keys, n, nm, L, q); }
 }
 void repack_keys(const uint64_t* in, KeyLayout A, uint64_t* out, KeyLayout B, int64_t n, int nm,
                  cudaStream_t s) {
-  if (n > 0) k_repack<<<grid_for(n, 256), 256, 0, s>>>(in, A, out, B, n, nm);
+  if (n > 0) { note_launch(); k_repack<<<grid_for(n, 256), 256, 0, s>>>(in, A, out, B, n, nm); }
 }
 void hash_clear(uint64_t* slots, uint64_t nslots, cudaStream_t s) {
-  k_fill_u64<<<grid_for((int64_t)nslots, 256), 256, 0, s>>>(slots, nslots, kEmptySlot);
+  note_launch(); k_fill_u64<<<grid_for((int64_t)nslots, 256), 256, 0, s>>>(slots, nslots, kEmptySlot);
 }
 void hash_insert_range(uint64_t* slots, uint64_t mask, const uint64_t* keys, int64_t begin,
                        int64_t end, int W, int* flags, cudaStream_t s) {
@@ -233,7 +239,7 @@ void hash_insert_range(uint64_t* slots, uint64_t mask, const uint64_t* keys, int
 void max_quanta_per_mode(const uint64_t* keys, int64_t n, int nm, KeyLayout L, int* out,
                          cudaStream_t s) {
   cudaMemsetAsync(out, 0, sizeof(int) * nm, s);
-  if (n > 0) k_max_quanta<<<grid_for(n, 256, 592), 256, 0, s>>>(keys, n, nm, L, out);
+  if (n > 0) { note_launch(); k_max_quanta<<<grid_for(n, 256, 592), 256, 0, s>>>(keys, n, nm, L, out); }
 }
 
 // ------------------------------------------------------------------------- heat-bath selection
@@ -320,7 +326,7 @@ template <int W>
 void select_gen_launch(const uint64_t* keys, int64_t n, const int64_t* woff, int64_t total,
                        HBTable hb, KeyLayout L, HashView basis, NewSetView ns, cudaStream_t s) {
   if (total <= 0) return;
-  k_select_gen<W><<<grid_for(total, 256, 148 * 32), 256, 0, s>>>(keys, n, woff, total, hb, L,
+  note_launch(); k_select_gen<W><<<grid_for(total, 256, 148 * 32), 256, 0, s>>>(keys, n, woff, total, hb, L,
                                                                 basis, ns);
 }
 
@@ -346,11 +352,11 @@ __global__ void k_compact(const uint64_t* __restrict__ cand, const uint8_t* __re
 }  // namespace
 
 void cmax_rows(const double* X, int64_t n, int ldx, int nopt, double* cmax, cudaStream_t s) {
-  if (n > 0) k_cmax<<<grid_for(n * 32, 256), 256, 0, s>>>(X, n, ldx, nopt, cmax);
+  if (n > 0) { note_launch(); k_cmax<<<grid_for(n * 32, 256), 256, 0, s>>>(X, n, ldx, nopt, cmax); }
 }
 void select_count(const double* cmax, int64_t n, HBTable hb, double eps, int64_t* work,
                   cudaStream_t s) {
-  if (n > 0) k_select_count<<<grid_for(n, 256), 256, 0, s>>>(cmax, n, hb, eps, work);
+  if (n > 0) { note_launch(); k_select_count<<<grid_for(n, 256), 256, 0, s>>>(cmax, n, hb, eps, work); }
 }
 void select_generate(const uint64_t* keys, int64_t n, const int64_t* woff, int64_t total,
                      HBTable hb, KeyLayout L, HashView basis, NewSetView ns, cudaStream_t s) {
@@ -360,7 +366,7 @@ void newset_compact(const uint64_t* cand, const uint8_t* dead, int64_t ncand, in
                     uint64_t* out, unsigned long long* n_out, cudaStream_t s) {
   cudaMemsetAsync(n_out, 0, sizeof(unsigned long long), s);
   if (ncand > 0)
-    k_compact<<<grid_for(ncand, 256), 256, 0, s>>>(cand, dead, ncand, W, out, n_out);
+    note_launch(); k_compact<<<grid_for(ncand, 256), 256, 0, s>>>(cand, dead, ncand, W, out, n_out);
 }
 
 // ------------------------------------------------------------------------------- radix sort ---
@@ -448,9 +454,9 @@ void radix_launch(uint64_t* keys, uint64_t* alt, int64_t n, int nbits, int64_t* 
   int passes = 0;
   for (int b = 0; b < nbits; b += 8) {
     const int word = b / 64, shift = b % 64;
-    k_radix_hist<W><<<nblk, kRadixThreads, 0, s>>>(src, n, word, shift, offs, nblk);
+    note_launch(); k_radix_hist<W><<<nblk, kRadixThreads, 0, s>>>(src, n, word, shift, offs, nblk);
     exclusive_scan(offs, offs, hn, tmp, s);
-    k_radix_scatter<W><<<nblk, kRadixThreads, 0, s>>>(src, dst, n, word, shift, offs, nblk);
+    note_launch(); k_radix_scatter<W><<<nblk, kRadixThreads, 0, s>>>(src, dst, n, word, shift, offs, nblk);
     uint64_t* t = src; src = dst; dst = t;
     ++passes;
   }

@@ -65,14 +65,14 @@ __global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ key
 template <int W>
 void hbuild_count_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
                          int32_t* rowcnt, cudaStream_t s) {
-  k_hbuild<W, false><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
+  note_launch(); k_hbuild<W, false><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
       keys, n, L, basis, cd, rowcnt, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 template <int W>
 void hbuild_fill_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
                         const int64_t* rowptr, int32_t* col, double* val, float* valf,
                         double* diag, cudaStream_t s) {
-  k_hbuild<W, true><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
+  note_launch(); k_hbuild<W, true><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
       keys, n, L, basis, cd, nullptr, rowptr, col, val, valf, diag);
 }
 
@@ -128,7 +128,7 @@ void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const V
   const int g = grid_for(n * 32, 256, 148 * 16);
   switch ((b + 31) / 32) {
 #define VHCI_SPMM_CASE(R) \
-  case R: k_spmm<R, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy); break;
+  case R: note_launch(); k_spmm<R, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy); break;
     VHCI_SPMM_CASE(1) VHCI_SPMM_CASE(2) VHCI_SPMM_CASE(3) VHCI_SPMM_CASE(4)
     VHCI_SPMM_CASE(5) VHCI_SPMM_CASE(6) VHCI_SPMM_CASE(7) VHCI_SPMM_CASE(8)
     VHCI_SPMM_CASE(9) VHCI_SPMM_CASE(10) VHCI_SPMM_CASE(11) VHCI_SPMM_CASE(12)
@@ -244,40 +244,40 @@ int residual_blocks(int64_t n) {
 
 void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,
                     const double* theta, double* part, int nblk, double* rn2, cudaStream_t s) {
-  k_resid_part<<<nblk, 256, 0, s>>>(X, HX, n, ld, kk, theta, part);
-  k_sum_parts<<<(kk + 255) / 256, 256, 0, s>>>(part, nblk, kk, rn2, 0);
+  note_launch(); k_resid_part<<<nblk, 256, 0, s>>>(X, HX, n, ld, kk, theta, part);
+  note_launch(); k_sum_parts<<<(kk + 255) / 256, 256, 0, s>>>(part, nblk, kk, rn2, 0);
 }
 
 void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
                          int64_t n, const int* cols, const double* theta, int nc, double* T,
                          int ldt, cudaStream_t s) {
   if (nc <= 0 || n <= 0) return;
-  k_correction<<<grid_for(n * nc, 256), 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, nc, T, ldt);
+  note_launch(); k_correction<<<grid_for(n * nc, 256), 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, nc, T, ldt);
 }
 
 void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,
                cudaStream_t s) {
   if (n <= 0 || ncol <= 0) return;
-  k_copy_cols<<<grid_for(n * ncol, 256), 256, 0, s>>>(src, lds, dst, ldd, n, ncol);
+  note_launch(); k_copy_cols<<<grid_for(n * ncol, 256), 256, 0, s>>>(src, lds, dst, ldd, n, ncol);
 }
 
 void dense_from_csr(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
                     const float* valf, const double* diag, double* A, cudaStream_t s) {
   fill_zero(A, n * n, s);
-  if (valf) k_dense_from_csr<float><<<grid_for(n, 128), 128, 0, s>>>(n, rowptr, col, valf, diag, A);
-  else k_dense_from_csr<double><<<grid_for(n, 128), 128, 0, s>>>(n, rowptr, col, val, diag, A);
+  if (valf) { note_launch(); k_dense_from_csr<float><<<grid_for(n, 128), 128, 0, s>>>(n, rowptr, col, valf, diag, A); }
+  else { note_launch(); k_dense_from_csr<double><<<grid_for(n, 128), 128, 0, s>>>(n, rowptr, col, val, diag, A); }
 }
 
 void fill_zero(double* p, int64_t n, cudaStream_t s) {
-  if (n > 0) k_fill_zero<<<grid_for(n, 256), 256, 0, s>>>(p, n);
+  if (n > 0) { note_launch(); k_fill_zero<<<grid_for(n, 256), 256, 0, s>>>(p, n); }
 }
 
 void set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr, cudaStream_t s) {
-  if (nr > 0) k_set_unit_rows<<<(nr + 127) / 128, 128, 0, s>>>(X, ldx, col0, rows, nr);
+  if (nr > 0) { note_launch(); k_set_unit_rows<<<(nr + 127) / 128, 128, 0, s>>>(X, ldx, col0, rows, nr); }
 }
 
 void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cudaStream_t s) {
-  k_sum_parts<<<(nopt + 255) / 256, 256, 0, s>>>(part, nblk, nopt, out_accum, 1);
+  note_launch(); k_sum_parts<<<(nopt + 255) / 256, 256, 0, s>>>(part, nblk, nopt, out_accum, 1);
 }
 
 }  // namespace vhci

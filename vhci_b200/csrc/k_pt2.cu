@@ -56,14 +56,14 @@ __global__ void __launch_bounds__(256) k_pt2_gen(const uint64_t* __restrict__ ke
 template <int W>
 void pt2_count_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
                       int64_t a_lo, int64_t a_hi, int32_t* acount, cudaStream_t s) {
-  k_pt2_gen<W, false><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
+  note_launch(); k_pt2_gen<W, false><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
       keys, n, L, pert, cd, a_lo, a_hi, acount, nullptr, nullptr, nullptr);
 }
 template <int W>
 void pt2_fill_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
                      int64_t a_lo, int64_t a_hi, const int64_t* arowptr, int32_t* afill,
                      int32_t* ecol, double* eval, cudaStream_t s) {
-  k_pt2_gen<W, true><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
+  note_launch(); k_pt2_gen<W, true><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
       keys, n, L, pert, cd, a_lo, a_hi, afill, arowptr, ecol, eval);
 }
 
@@ -140,7 +140,7 @@ void pt2_en_launch(const uint64_t* pkeys, int64_t a_lo, int64_t a_hi, KeyLayout 
   switch ((nopt + 31) / 32) {
 #define VHCI_EN_CASE(R)                                                                        \
   case R:                                                                                      \
-    k_pt2_en<W, R><<<kEnBlocks, kEnThreads, 0, s>>>(pkeys, a_lo, a_hi, L, cd, arowptr, ecol, \
+    note_launch(); k_pt2_en<W, R><<<kEnBlocks, kEnThreads, 0, s>>>(pkeys, a_lo, a_hi, L, cd, arowptr, ecol, \
                                                     eval, X, ldx, nopt, E, part);            \
     break;
     VHCI_EN_CASE(1) VHCI_EN_CASE(2) VHCI_EN_CASE(3) VHCI_EN_CASE(4)

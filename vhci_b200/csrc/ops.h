@@ -8,6 +8,10 @@
 
 namespace vhci {
 
+// Process-wide count of this library's kernel launches (reported in vhci_stats).
+void note_launch();
+long long launch_count();
+
 // ---- device table records ----
 struct GroupDev {   // one connection group (a fixed quanta change)
   int32_t tb, te;   // term range

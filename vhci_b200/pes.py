@@ -26,6 +26,16 @@ binary and the GPU build all read one identical file.  Every draw comes from one
   (multisets with at most two distinct modes, i^6 and i^a j^(6-a), keep p6, positive).
 
 Values are written with 10 decimals, so every reader parses the same doubles.
+
+Admissibility.  Independent random cubic/quartic terms often make the potential fall below its
+expansion minimum a few quanta out (e.g. a large cubic term on a soft mode with no diagonal
+quartic).  Heat-bath selection then walks into that region and the variational energy collapses
+without converging — the reference procedure does the same on such a surface.  A workload
+therefore uses the first draw, over seeds base + 100*j (j = 0, 1, ...), whose potential is
+non-negative on every one- and two-mode plane within |q| <= sqrt(2*16+1) and on every three-mode
+cube within |q| <= sqrt(2*12+1) (dimensionless normal coordinates, V = sum w q^2/2 +
+sum phi/prod(p_k!) prod q^p_k, i.e. the region spanned by up to 16 resp. 12 quanta per mode).
+`admissible()` implements the test and `CONFIG_SEED_OFFSET` records the first accepted j.
 """
 from __future__ import annotations
 
@@ -127,13 +137,75 @@ CONFIGS = {
 }
 
 
+# First admissible draw j (seed = base + 100*j) per workload, found with `find_admissible`.
+CONFIG_SEED_OFFSET = {0: 0, 1: 1, 2: 0, 4: 0}
+
+
 def config_seed(config: int, request: int = 0) -> int:
     return SEED_BASE + config * 1000 + request
 
 
-def write_config(path: str, config: int, run: RunSettings | None = None, request: int = 0) -> None:
+def workload_seed(config: int) -> int:
+    return config_seed(config) + 100 * CONFIG_SEED_OFFSET.get(config, 0)
+
+
+def _subset_terms(pes: PES):
+    """FC terms keyed by their mode set: list of (modes, powers, coefficient / prod p!)."""
+    from math import factorial
+    out = {}
+    for ms, v in pes.fcs:
+        modes = tuple(sorted(set(ms)))
+        pw = tuple(ms.count(m) for m in modes)
+        den = 1.0
+        for p in pw:
+            den *= factorial(p)
+        out.setdefault(modes, []).append((modes, pw, v / den))
+    return out
+
+
+def _min_potential(pes: PES, terms, modes, qmax, ng):
+    g = np.linspace(-qmax, qmax, ng)
+    grids = np.meshgrid(*([g] * len(modes)), indexing="ij")
+    q = {m: grids[i].ravel() for i, m in enumerate(modes)}
+    V = np.zeros(grids[0].size)
+    for m in modes:
+        V += 0.5 * pes.freqs[m] * q[m] ** 2
+    for r in range(1, len(modes) + 1):
+        for sub in itertools.combinations(modes, r):
+            for tm, pw, c in terms.get(sub, ()):
+                t = np.full(V.shape, c)
+                for m, p in zip(tm, pw):
+                    t = t * q[m] ** p
+                V += t
+    return float(V.min())
+
+
+def admissible(pes: PES, pair_quanta: int = 16, triple_quanta: int = 12) -> bool:
+    """Potential >= 0 on all one/two-mode planes and three-mode cubes of the stated extent."""
+    terms = _subset_terms(pes)
+    nm = len(pes.freqs)
+    q2 = math.sqrt(2 * pair_quanta + 1)
+    q3 = math.sqrt(2 * triple_quanta + 1)
+    for i, j in itertools.combinations(range(nm), 2):
+        if _min_potential(pes, terms, (i, j), q2, 41) < 0:
+            return False
+    for tri in itertools.combinations(range(nm), 3):
+        if _min_potential(pes, terms, tri, q3, 13) < 0:
+            return False
+    return True
+
+
+def find_admissible(config: int, max_tries: int = 50) -> int:
+    spec, _ = CONFIGS[config]
+    for j in range(max_tries):
+        if admissible(generate(spec, config_seed(config) + 100 * j)):
+            return j
+    raise RuntimeError(f"no admissible draw for workload {config} in {max_tries} tries")
+
+
+def write_config(path: str, config: int, run: RunSettings | None = None) -> None:
     spec, default_run = CONFIGS[config]
-    pes = generate(spec, config_seed(config, request))
+    pes = generate(spec, workload_seed(config))
     write_input(path, pes, run or default_run, comment=f"synthetic PES, workload {config}")
 
 
