@@ -150,6 +150,10 @@ vhci_status vhci_get_h_csr(const vhci_ctx* c, int64_t* rowptr, int32_t* col, dou
  * for the "% sparse" line (Ham.cpp:341-342). */
 vhci_status vhci_structural_nnz(vhci_ctx* c, int64_t* nnz);
 
+/* Y = H X for b host vectors (n x b, column-major) with the current Hamiltonian (built on first
+ * use): the sparse product the eigensolver runs (SparseSymMatProd in the reference, Ham.cpp:349). */
+vhci_status vhci_apply_h(vhci_ctx* c, const double* X, double* Y, int b);
+
 /* Lowest k eigenpairs of the current Hamiltonian (SparseDiagonalize, Ham.cpp:347-370; dense
  * eigensolve for small bases, DenseDiagonalize, :372-379).  Vectors stay on device; E (k)
  * receives the eigenvalues if not NULL. */

@@ -135,6 +135,34 @@ def test_end_to_end_vs_reference_outputs(api, case):
         assert r["n_pert"] == g["log"]["n_pert"]
 
 
+def test_davidson_end_to_end_workload0(api):
+    """Workload 0 (12 modes, 35,229 states, Nstate 50): the sparse eigensolver path end to end
+    against the reference program's own output."""
+    g = load_golden("workload0")
+    r = api.solve(g["input"])
+    lev = levels_of(r["E"])
+    ref = np.array(g["levels"])
+    assert np.abs(lev[:len(ref)] - ref).max() <= E_TOL
+    assert r["n_basis"] == g["log"]["final_basis"]
+
+
+@pytest.mark.parametrize("b", [1, 5, 8, 13, 16, 31, 40, 97])
+def test_spmm_matches_csr_product(api, b):
+    """H X on the device (all column-panel widths) against the CSR product of the same matrix."""
+    g = load_golden("syn_m8_sextic_pt2")
+    o = O.Oracle(g["input"])
+    w, C = _oracle_first_step(o)
+    o.append_basis(o.select(C, min(o.neig, o.n), o.eps1))
+    rng = np.random.default_rng(b)
+    with api.VHCI(g["input"]) as v:
+        v.set_basis(o.basis().astype(np.uint8))
+        H = v.h_csr()
+        X = rng.standard_normal((v.n, b))
+        Y = v.apply_h(X)
+    ref = H @ X
+    assert np.abs(Y - ref).max() <= 1e-12 * np.abs(H).sum(axis=1).max() * np.abs(X).max()
+
+
 def test_key_layout_8bit_for_high_quanta(api):
     g = load_golden("clo2_vci")  # Max_quanta 25 needs 8-bit mode fields
     with api.VHCI(g["input"]) as v:

@@ -26,7 +26,7 @@ EXPORTS = [
     "vhci_get_hb_list", "vhci_get_freqs", "vhci_set_basis", "vhci_get_basis", "vhci_set_vectors",
     "vhci_get_vectors", "vhci_select", "vhci_get_selected", "vhci_build_h", "vhci_get_h_csr",
     "vhci_structural_nnz", "vhci_eigs", "vhci_hci", "vhci_pt2", "vhci_write_freqs",
-    "vhci_write_checkpoint", "vhci_read_checkpoint", "vhci_get_energies",
+    "vhci_write_checkpoint", "vhci_read_checkpoint", "vhci_get_energies", "vhci_apply_h",
 ]
 
 
@@ -114,6 +114,7 @@ def lib():
             "vhci_get_h_csr": (ctypes.c_int, [vp, i64p, i32p, dp]),
             "vhci_structural_nnz": (ctypes.c_int, [vp, i64p]),
             "vhci_eigs": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+            "vhci_apply_h": (ctypes.c_int, [vp, dp, dp, ctypes.c_int]),
             "vhci_hci": (ctypes.c_int, [vp, ctypes.c_char_p, vp, vp]),
             "vhci_pt2": (ctypes.c_int, [vp, ctypes.c_double, dp, i64p]),
             "vhci_write_freqs": (ctypes.c_int, [vp, ctypes.c_char_p]),
@@ -288,6 +289,13 @@ class VHCI:
         self._check(lib().vhci_get_h_csr(self.h, _ptr(rp, ctypes.c_int64), _ptr(col, ctypes.c_int32),
                                          _ptr(val, ctypes.c_double)))
         return sp.csr_matrix((val, col, rp), shape=(n, n))
+
+    def apply_h(self, X: np.ndarray) -> np.ndarray:
+        X = np.asfortranarray(X, np.float64)
+        Y = np.zeros_like(X, order="F")
+        self._check(lib().vhci_apply_h(self.h, _ptr(X, ctypes.c_double), _ptr(Y, ctypes.c_double),
+                                       X.shape[1]))
+        return Y
 
     def eigs(self, k: int) -> np.ndarray:
         E = np.zeros(k)

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -119,13 +120,14 @@ int svqb(vhci_ctx* c, Work& w, int64_t n, const double* B, int ld, int nb, doubl
   return VHCI_OK;
 }
 
-// B (nb cols, ld) -= V[:, 0:m] (V^T B), twice (classical Gram-Schmidt with reorthogonalisation).
+// B (nb cols, ld) -= V[:, 0:m] (V^T B), `passes` times (classical Gram-Schmidt; the Davidson
+// step interleaves single passes with SVQB, which together re-orthogonalise).
 int project_out(vhci_ctx* c, Work& w, int64_t n, const double* V, int ldv, int m, double* B,
-                int ld, int nb) {
+                int ld, int nb, int passes = 2) {
   if (m <= 0 || nb <= 0) return VHCI_OK;
   const double one = 1.0, zero = 0.0, mone = -1.0;
   VCK(w.S.reserve((size_t)m * nb, c->st));
-  for (int pass = 0; pass < 2; ++pass) {
+  for (int pass = 0; pass < passes; ++pass) {
     VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, nb, (int)n, &one, V, ldv, B, ld, &zero,
                     w.S.p, m));
     VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, (int)n, m, &mone, w.S.p, m, V, ldv,
@@ -384,11 +386,13 @@ int davidson(vhci_ctx* c, int k) {
       have_prev = true;
     }
     VCK(h2d(c, w.cols.p, cols.data(), nc * sizeof(int)));
-    davidson_correction(w.Xn.p, w.HXn.p, kk, c->diag.p, n, w.cols.p, w.theta.p, nc, w.Tb.p, kk, s);
-    VTRY(project_out(c, w, n, w.V.p, mmax, m, w.Tb.p, kk, nc));
+    VCK(w.part.reserve(std::max<size_t>((size_t)nblk * kk, (size_t)correction_scratch(n, nc)), s, false));
+    davidson_correction(w.Xn.p, w.HXn.p, kk, c->diag.p, n, w.cols.p, w.theta.p, nc, w.Tb.p, kk,
+                        w.part.p, s);
+    VTRY(project_out(c, w, n, w.V.p, mmax, m, w.Tb.p, kk, nc, 1));
     int r = 0;
     VTRY(svqb(c, w, n, w.Tb.p, kk, nc, w.Tb2.p, kk, &r));
-    VTRY(project_out(c, w, n, w.V.p, mmax, m, w.Tb2.p, kk, r));
+    VTRY(project_out(c, w, n, w.V.p, mmax, m, w.Tb2.p, kk, r, 1));
     int r2 = 0;
     VTRY(svqb(c, w, n, w.Tb2.p, kk, r, w.V.p + m, mmax, &r2));
     if (r2 == 0) return fail(c, VHCI_E_NOT_CONVERGED, "Davidson stagnated (no new directions)");
@@ -440,8 +444,10 @@ int eigs(vhci_ctx* c, int k) {
   const int kk = (int)std::min<int64_t>(n, k + guard);
   VCK(cudaEventRecord(c->ev_a, c->st));
   int r;
+  const char* which = std::getenv("VHCI_EIGS");
   if (n <= 2000 || n <= 3 * (int64_t)kk + 64) r = dense_eigs(c, kk);
-  else r = davidson(c, k);
+  else if (which && std::string(which) == "davidson") r = davidson(c, k);
+  else r = block_lanczos(c, k);
   if (r != VHCI_OK) return r;
   VCK(cudaEventRecord(c->ev_b, c->st));
   VCK(cudaEventSynchronize(c->ev_b));
@@ -452,6 +458,27 @@ int eigs(vhci_ctx* c, int k) {
 }  // namespace vhci
 
 using namespace vhci;
+
+extern "C" vhci_status vhci_apply_h(vhci_ctx* c, const double* X, double* Y, int b) {
+  if (!c || !X || !Y || b <= 0) return VHCI_E_INPUT;
+  if (!c->h_valid) VTRY(build_h(c));
+  const int64_t n = c->n;
+  std::vector<double> h((size_t)n * b);
+  for (int64_t i = 0; i < n; ++i)
+    for (int j = 0; j < b; ++j) h[(size_t)i * b + j] = X[(size_t)j * n + i];
+  DBuf<double> dx, dy;
+  VCK(dx.reserve(h.size(), c->st));
+  VCK(dy.reserve(h.size(), c->st));
+  VCK(h2d(c, dx.p, h.data(), h.size() * sizeof(double)));
+  VTRY(apply_h(c, dx.p, b, b, dy.p, b));
+  VCK(d2h(c, h.data(), dy.p, h.size() * sizeof(double)));
+  VCK(cudaStreamSynchronize(c->st));
+  dx.release(c->st);
+  dy.release(c->st);
+  for (int64_t i = 0; i < n; ++i)
+    for (int j = 0; j < b; ++j) Y[(size_t)j * n + i] = h[(size_t)i * b + j];
+  return VHCI_OK;
+}
 
 extern "C" vhci_status vhci_eigs(vhci_ctx* c, int k, double* E) {
   if (!c || k <= 0) return VHCI_E_INPUT;

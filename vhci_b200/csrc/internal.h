@@ -46,6 +46,9 @@ int build_h(vhci_ctx* c);
 // Lowest k eigenpairs; dense_all keeps every eigenpair of a dense solve (first HCI step).
 int eigs(vhci_ctx* c, int k);
 int dense_eigs(vhci_ctx* c, int keep);
+// Block thick-restart Lanczos (lanczos.cu).
+int block_lanczos(vhci_ctx* c, int k);
+int lanczos_block(int64_t n);
 int pt2(vhci_ctx* c, double eps2, double* dE, int64_t* n_pert);
 
 float event_ms(vhci_ctx* c);

@@ -1,5 +1,7 @@
 // Hamiltonian kernels: the connection-driven sparse build (replacing the reference's O(N^2) pair
 // loop, Ham.cpp:228-326), the SpMM that drives the eigensolver, and the Davidson vector helpers.
+#include <algorithm>
+
 #include "conn.cuh"
 #include "ops.h"
 
@@ -121,11 +123,71 @@ __global__ void __launch_bounds__(256) k_spmm(int64_t n, const int64_t* __restri
   }
 }
 
+// One column panel Y[:, 0:bp] = (D + H_off) X[:, 0:bp], bp <= BP.  A warp handles one row; its
+// lanes form S = 32/BP entry slots of BP lanes (slot s takes entries s, s+S, ...), each lane owns
+// one column, and the slots are summed with shuffles at the end.  The launcher keeps the panel's
+// X columns (n * bp * 8 bytes) within the L2 budget so the per-entry gathers hit L2 while the
+// matrix streams from HBM once per panel.
+template <int BP, typename VT>
+__global__ void __launch_bounds__(256) k_spmm_panel(int64_t n, const int64_t* __restrict__ rowptr,
+                                                    const int32_t* __restrict__ col,
+                                                    const VT* __restrict__ val,
+                                                    const double* __restrict__ diag,
+                                                    const double* __restrict__ X, int ldx, int bp,
+                                                    double* __restrict__ Y, int ldy) {
+  constexpr int S = 32 / BP;
+  const int lane = threadIdx.x & 31;
+  const int slot = lane / BP, cc = lane % BP;
+  const bool active = cc < bp;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += warps) {
+    double acc = 0.0;
+    const int64_t beg = rowptr[i], end = rowptr[i + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      int jj = 0;
+      double vv = 0.0;
+      if (e < end) { jj = __ldcs(col + e); vv = (double)__ldcs(val + e); }
+      const int m = (int)(end - e0 < 32 ? end - e0 : 32);
+#pragma unroll 4
+      for (int t = 0; t < m; t += S) {
+        const int src = t + slot;
+        const int j = __shfl_sync(0xffffffffu, jj, src & 31);
+        const double v = __shfl_sync(0xffffffffu, vv, src & 31);
+        if (active && src < m) acc = fma(v, __ldg(X + (int64_t)j * ldx + cc), acc);
+      }
+    }
+#pragma unroll
+    for (int o = BP; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (slot == 0 && active) Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
+  }
+}
+
+// L2 budget for one panel of gathered vector columns (bytes); B200 has 126 MB of L2.
+constexpr double kSpmmL2Budget = 64e6;
+
 template <typename VT>
 void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
                    const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
                    cudaStream_t s) {
   const int g = grid_for(n * 32, 256, 148 * 16);
+  // L2 holds whole 128-byte lines: a panel of BP columns occupies n * max(128, 8 BP) bytes
+  const double lines = (double)n * 128.0;
+  if (lines * ((b + 15) / 16) > kSpmmL2Budget || b <= 16) {
+    // column panels: 32 columns when two lines per row fit the budget, else 16 (one line per row;
+    // 8 only for blocks of at most 8 columns)
+    int BP = (lines * 2 <= kSpmmL2Budget) ? 32 : 16;
+    if (b <= 8) BP = 8;
+    else if (b <= 16) BP = 16;
+    for (int c0 = 0; c0 < b; c0 += BP) {
+      const int bp = std::min(BP, b - c0);
+      if (BP == 32) { note_launch(); k_spmm_panel<32, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      else if (BP == 16) { note_launch(); k_spmm_panel<16, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      else { note_launch(); k_spmm_panel<8, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+    }
+    return;
+  }
   switch ((b + 31) / 32) {
 #define VHCI_SPMM_CASE(R) \
   case R: note_launch(); k_spmm<R, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy); break;
@@ -162,21 +224,66 @@ __global__ void k_sum_parts(const double* __restrict__ part, int nblk, int kk,
   }
 }
 
+__device__ __forceinline__ double precond_den(double th, double d) {
+  double den = th - d;
+  const double g = 1e-6 * fmax(1.0, fabs(th));
+  if (fabs(den) < g) den = den < 0 ? -g : g;
+  return den;
+}
+
+// Per-block partial sums for Olsen's correction: a_j = sum_i x_i r_i / (theta_j - D_i),
+// b_j = sum_i x_i^2 / (theta_j - D_i) over this block's rows.
+__global__ void k_olsen_part(const double* __restrict__ X, const double* __restrict__ HX, int ldx,
+                             const double* __restrict__ diag, int64_t n,
+                             const int* __restrict__ cols, const double* __restrict__ theta,
+                             int nc, double* __restrict__ part) {
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = blockIdx.x * per, hi = min(n, lo + per);
+  for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+    const int c = cols[j];
+    const double th = theta[c];
+    double a = 0.0, b = 0.0;
+    for (int64_t i = lo; i < hi; ++i) {
+      const double x = X[i * ldx + c];
+      const double r = HX[i * ldx + c] - th * x;
+      const double den = precond_den(th, diag[i]);
+      a += x * r / den;
+      b += x * x / den;
+    }
+    part[(int64_t)blockIdx.x * 2 * nc + j] = a;
+    part[(int64_t)blockIdx.x * 2 * nc + nc + j] = b;
+  }
+}
+
+__global__ void k_olsen_eps(const double* __restrict__ part, int nblk, int nc,
+                            double* __restrict__ eps) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nc; j += gridDim.x * blockDim.x) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < nblk; ++q) {
+      a += part[(int64_t)q * 2 * nc + j];
+      b += part[(int64_t)q * 2 * nc + nc + j];
+    }
+    eps[j] = (fabs(b) > 1e-300) ? a / b : 0.0;
+  }
+}
+
+// t_i = (r_i - eps_j x_i) / (theta_j - D_i): the diagonal-preconditioned residual made orthogonal
+// to the Ritz vector in the preconditioner's metric (Olsen's correction), which keeps Davidson
+// from stalling when the plain correction turns parallel to the Ritz vector.
 __global__ void k_correction(const double* __restrict__ X, const double* __restrict__ HX, int ldx,
                              const double* __restrict__ diag, int64_t n,
                              const int* __restrict__ cols, const double* __restrict__ theta,
-                             int nc, double* __restrict__ T, int ldt) {
+                             const double* __restrict__ eps, int nc, double* __restrict__ T,
+                             int ldt) {
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n * nc;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = idx / nc;
     const int j = (int)(idx % nc);
     const int c = cols[j];
     const double th = theta[c];
-    const double r = HX[i * ldx + c] - th * X[i * ldx + c];
-    double den = th - diag[i];
-    const double g = 1e-6 * fmax(1.0, fabs(th));
-    if (fabs(den) < g) den = den < 0 ? -g : g;
-    T[i * ldt + j] = r / den;
+    const double x = X[i * ldx + c];
+    const double r = HX[i * ldx + c] - th * x;
+    T[i * ldt + j] = (r - eps[j] * x) / precond_den(th, diag[i]);
   }
 }
 
@@ -248,11 +355,17 @@ void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk
   note_launch(); k_sum_parts<<<(kk + 255) / 256, 256, 0, s>>>(part, nblk, kk, rn2, 0);
 }
 
+int correction_scratch(int64_t n, int nc) { return residual_blocks(n) * 2 * nc + nc; }
+
 void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
                          int64_t n, const int* cols, const double* theta, int nc, double* T,
-                         int ldt, cudaStream_t s) {
+                         int ldt, double* scratch, cudaStream_t s) {
   if (nc <= 0 || n <= 0) return;
-  note_launch(); k_correction<<<grid_for(n * nc, 256), 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, nc, T, ldt);
+  const int nblk = residual_blocks(n);
+  double* eps = scratch + (int64_t)nblk * 2 * nc;
+  note_launch(); k_olsen_part<<<nblk, 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, nc, scratch);
+  note_launch(); k_olsen_eps<<<(nc + 255) / 256, 256, 0, s>>>(scratch, nblk, nc, eps);
+  note_launch(); k_correction<<<grid_for(n * nc, 256), 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, eps, nc, T, ldt);
 }
 
 void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,

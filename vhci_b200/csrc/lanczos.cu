@@ -1,0 +1,360 @@
+// Block thick-restart Lanczos for the lowest eigenpairs of the sparse Hamiltonian — the same
+// method family as the reference's eigensolver (implicitly restarted Lanczos, SparseDiagonalize,
+// Ham.cpp:347-370), organised for the GPU:
+//   * blocks of b = 16 or 32 vectors (sized so the block's 128-byte L2 lines stay resident), so the
+//     SpMM streams the matrix from HBM once per block while the per-entry gathers hit L2;
+//   * full reorthogonalisation (classical Gram-Schmidt, two passes) with FP64 GEMMs, and the
+//     projected matrix T = Q^T H Q formed explicitly from the stored H Q blocks;
+//   * Rayleigh-Ritz (cuSOLVER syevd on T) only when the subspace is full; the kk = k + guard
+//     lowest Ritz vectors are kept (thick restart) together with the pending Lanczos block, so the
+//     kept Ritz vectors' residuals lie in the new subspace (Krylov-Schur property);
+//   * convergence: ||H x - theta x|| <= tol * max(eps^(2/3), |theta|) for the k wanted pairs,
+//     evaluated with explicit residuals at each restart (tol 1e-10 in the reference);
+//   * heat-bath iterations start from b random combinations of the previous Ritz vectors
+//     (zero-extended over the new states).
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "internal.h"
+
+namespace vhci {
+
+namespace {
+
+// Cyclic Jacobi eigensolver for a small symmetric matrix (column-major, n <= 64): eigenvalues
+// ascending in w, eigenvectors in the columns of V.
+void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std::vector<double>& V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+  auto a = [&](int i, int j) -> double& { return A[(size_t)j * n + i]; };
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        tot += a(i, j) * a(i, j);
+        if (i != j) off += a(i, j) * a(i, j);
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a(p, q);
+        if (std::fabs(apq) < 1e-300) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = cs * akp - sn * akq;
+          a(k, q) = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = cs * apk - sn * aqk;
+          a(q, k) = sn * apk + cs * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[(size_t)p * n + k], vkq = V[(size_t)q * n + k];
+          V[(size_t)p * n + k] = cs * vkp - sn * vkq;
+          V[(size_t)q * n + k] = sn * vkp + cs * vkq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  std::vector<double> V2((size_t)n * n);
+  w.resize(n);
+  for (int j = 0; j < n; ++j) {
+    w[j] = a(ord[j], ord[j]);
+    for (int i = 0; i < n; ++i) V2[(size_t)j * n + i] = V[(size_t)ord[j] * n + i];
+  }
+  V.swap(V2);
+}
+
+struct LWork {
+  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2;
+  void release(cudaStream_t s) {
+    Q.release(s); HQ.release(s); T.release(s); Yw.release(s); theta.release(s); Xb.release(s);
+    HXb.release(s); W.release(s); S.release(s); M.release(s); part.release(s); rn2.release(s);
+  }
+};
+
+int syevd_l(vhci_ctx* c, double* A, int m, int lda, double* w) {
+  int lwork = 0;
+  VBL(cusolverDnDsyevd_bufferSize(c->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m, A,
+                                  lda, w, &lwork));
+  VCK(c->solver_work.reserve(std::max(lwork, 1), c->st));
+  VCK(c->solver_info.reserve(1, c->st));
+  VBL(cusolverDnDsyevd(c->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m, A, lda, w,
+                       c->solver_work.p, lwork, c->solver_info.p));
+  int info = 0;
+  VCK(d2h(c, &info, c->solver_info.p, sizeof(int)));
+  VCK(cudaStreamSynchronize(c->st));
+  if (info != 0) return fail(c, VHCI_E_NOT_CONVERGED, "projected eigensolve failed");
+  return VHCI_OK;
+}
+
+// Orthonormalise the nb columns of (B, ld) into (out, ldo) by SVQB with the small Gram matrix
+// decomposed on the host; directions below 1e-12 of the largest are dropped.  *r = rank.
+int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb, double* out,
+               int ldo, int* r) {
+  *r = 0;
+  if (nb <= 0) return VHCI_OK;
+  const double one = 1.0, zero = 0.0;
+  VCK(w.S.reserve((size_t)nb * nb, c->st));
+  VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, (int)n, &one, B, ld, B, ld, &zero,
+                  w.S.p, nb));
+  std::vector<double> S((size_t)nb * nb);
+  VCK(d2h(c, S.data(), w.S.p, S.size() * sizeof(double)));
+  VCK(cudaStreamSynchronize(c->st));
+  std::vector<double> d(nb);
+  double dmax = 0.0;
+  for (int i = 0; i < nb; ++i) dmax = std::max(dmax, S[(size_t)i * nb + i]);
+  for (int i = 0; i < nb; ++i) {
+    const double s = S[(size_t)i * nb + i];
+    d[i] = (s > 1e-28 * dmax && s > 1e-300) ? 1.0 / std::sqrt(s) : 0.0;
+  }
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) S[(size_t)j * nb + i] *= d[i] * d[j];
+  std::vector<double> L, U;
+  jacobi_eig(nb, S, L, U);
+  const double lmax = L[nb - 1];
+  std::vector<int> keep;
+  for (int j = nb - 1; j >= 0; --j)
+    if (L[j] > 1e-12 * lmax && L[j] > 0) keep.push_back(j);
+  const int rr = (int)keep.size();
+  if (rr == 0) return VHCI_OK;
+  std::vector<double> Mh((size_t)nb * rr);
+  for (int q = 0; q < rr; ++q) {
+    const double s = 1.0 / std::sqrt(L[keep[q]]);
+    for (int i = 0; i < nb; ++i) Mh[(size_t)q * nb + i] = d[i] * U[(size_t)keep[q] * nb + i] * s;
+  }
+  VCK(w.M.reserve(Mh.size(), c->st));
+  VCK(h2d(c, w.M.p, Mh.data(), Mh.size() * sizeof(double)));
+  VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, rr, (int)n, nb, &one, w.M.p, nb, B, ld, &zero,
+                  out, ldo));
+  *r = rr;
+  return VHCI_OK;
+}
+
+int apply_h_l(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
+  cudaEvent_t e0, e1;
+  VCK(cudaEventCreate(&e0));
+  VCK(cudaEventCreate(&e1));
+  VCK(cudaEventRecord(e0, c->st));
+  spmm(c->n, c->rowptr.p, c->col.p, c->o.precision == 1 ? nullptr : c->val.p,
+       c->o.precision == 1 ? c->valf.p : nullptr, c->diag.p, X, ldx, b, Y, ldy, c->st);
+  VCK(cudaEventRecord(e1, c->st));
+  VCK(cudaEventSynchronize(e1));
+  VCK(cudaGetLastError());
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->stats.ms_spmm += ms;
+  c->stats.spmm_calls += 1;
+  c->stats.spmm_cols += b;
+  const int64_t sval = c->o.precision == 1 ? 4 : 8;
+  c->stats.spmm_bytes += c->nnz * (sval + 4) + (c->n + 1) * 8 + c->n * 8 + 2 * c->n * (int64_t)b * 8;
+  return VHCI_OK;
+}
+
+}  // namespace
+
+// Block size for a basis of n states: 32 when the block's L2 lines (two 128-byte lines per row)
+// fit 64 MB, else 16 (one line per row, the narrowest block that uses whole lines).
+int lanczos_block(int64_t n) { return (double)n * 256.0 <= 64e6 ? 32 : 16; }
+
+int block_lanczos(vhci_ctx* c, int k) {
+  const int64_t n = c->n;
+  cudaStream_t s = c->st;
+  const int guard = std::max(8, k / 10);
+  const int kk = (int)std::min<int64_t>(n, k + guard);
+  const int b = lanczos_block(n);
+  const int mmax = (int)std::min<int64_t>(n, (int64_t)3 * kk + 2 * b);
+  // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
+  const int ld = (mmax + b + 15) / 16 * 16;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  const double tol = c->o.eig_tol > 0 ? c->o.eig_tol : 1e-10;
+  const double eps23 = std::pow(DBL_EPSILON, 2.0 / 3.0);
+  const char* prof = std::getenv("VHCI_PROFILE");
+  const int plevel = prof ? std::atoi(prof) : 0;
+  LWork w;
+  VCK(w.Q.reserve((size_t)n * ld, s));
+  VCK(w.HQ.reserve((size_t)n * ld, s));
+  VCK(w.T.reserve((size_t)ld * ld, s));
+  VCK(w.Yw.reserve((size_t)ld * ld, s));
+  VCK(w.theta.reserve(ld, s));
+  VCK(w.Xb.reserve((size_t)n * kk, s));
+  VCK(w.HXb.reserve((size_t)n * kk, s));
+  VCK(w.W.reserve((size_t)n * b, s));
+  const int nblk = residual_blocks(n);
+  VCK(w.part.reserve((size_t)nblk * kk, s));
+  VCK(w.rn2.reserve(kk, s));
+  fill_zero(w.Q.p, n * (int64_t)ld, s);
+  VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
+
+  // ---- start block: random combinations of the previous Ritz vectors, else random vectors
+  std::vector<double> rnd;
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  auto urand = [&]() {
+    st = mix64(st + 0x632BE59BD9B4E019ull);
+    return ((st >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  };
+  auto nrand = [&]() { return std::sqrt(-2.0 * std::log(urand())) * std::cos(6.283185307179586 * urand()); };
+  int m = 0, p = 0;
+  if (c->nvec > 0 && c->x_rows > 0 && c->x_rows <= n) {
+    // start block = X0 R (random R, w0 x b), zero on the new states: the Krylov space it
+    // generates contains the previous Ritz vectors after about w0/b steps, and the Krylov-Schur
+    // relation holds from the first step on
+    const int w0 = std::min(c->nvec, kk);
+    rnd.resize((size_t)w0 * b);
+    for (auto& x : rnd) x = nrand();
+    DBuf<double> R;
+    VCK(R.reserve(rnd.size(), s));
+    VCK(h2d(c, R.p, rnd.data(), rnd.size() * sizeof(double)));
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, b, (int)c->x_rows, w0, &one, R.p, w0, c->X.p,
+                    c->ldx, &zero, w.W.p, b));
+    if (c->x_rows < n) fill_zero(w.W.p + (size_t)c->x_rows * b, (n - c->x_rows) * (int64_t)b, s);
+    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    VCK(cudaStreamSynchronize(s));
+    R.release(s);
+    if (p == 0) return fail(c, VHCI_E_NOT_CONVERGED, "empty start block");
+  } else {
+    rnd.resize((size_t)n * b);
+    for (auto& x : rnd) x = nrand();
+    VCK(h2d(c, w.W.p, rnd.data(), rnd.size() * sizeof(double)));
+    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    if (p == 0) return fail(c, VHCI_E_NOT_CONVERGED, "empty start block");
+  }
+
+  std::vector<double> th(ld), rn(kk);
+  const int maxcyc = c->o.eig_maxit > 0 ? c->o.eig_maxit : 1000;
+  auto t_start = std::chrono::steady_clock::now();
+  double t_spmm = 0, t_orth = 0, t_rr = 0;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto msince = [&](std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(now() - t0).count();
+  };
+  int steps = 0;
+  for (int cyc = 0; cyc < maxcyc; ++cyc) {
+    // ---- expansion
+    bool exhausted = (p == 0);
+    while (p > 0) {
+      auto t0 = now();
+      VTRY(apply_h_l(c, w.Q.p + m, ld, p, w.HQ.p + m, ld));
+      t_spmm += msince(t0);
+      t0 = now();
+      ++steps;
+      // T[0:m+p, m:m+p] = Q^T (H Q_new)
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m + p, p, (int)n, &one, w.Q.p, ld,
+                      w.HQ.p + m, ld, &zero, w.T.p + (size_t)m * ld, ld));
+      m += p;
+      if (m + b > mmax || m >= n) {
+        if (plevel) { cudaStreamSynchronize(s); t_orth += msince(t0); }
+        break;
+      }
+      // next block: W = H Q_new - Q T[:, new]; second Gram-Schmidt pass; SVQB
+      copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, n, p, s);
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.T.p + (size_t)(m - p) * ld,
+                      ld, w.Q.p, ld, &one, w.W.p, b));
+      VCK(w.S.reserve((size_t)m * p, s));
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, p, (int)n, &one, w.Q.p, ld, w.W.p, b,
+                      &zero, w.S.p, m));
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.S.p, m, w.Q.p, ld,
+                      &one, w.W.p, b));
+      int p2 = 0;
+      VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + m, ld, &p2));
+      t_orth += msince(t0);
+      p = p2;
+      if (p == 0) { exhausted = true; break; }
+    }
+    // ---- Rayleigh-Ritz on T[0:m, 0:m]
+    auto t0 = now();
+    c->stats.eig_iterations += 1;
+    VCK(cudaMemcpy2DAsync(w.Yw.p, ld * sizeof(double), w.T.p, ld * sizeof(double),
+                          m * sizeof(double), m, cudaMemcpyDeviceToDevice, s));
+    VTRY(syevd_l(c, w.Yw.p, m, ld, w.theta.p));
+    const int nk = std::min(kk, m);
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nk, (int)n, m, &one, w.Yw.p, ld, w.Q.p, ld,
+                    &zero, w.Xb.p, kk));
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nk, (int)n, m, &one, w.Yw.p, ld, w.HQ.p, ld,
+                    &zero, w.HXb.p, kk));
+    residual_norms(w.Xb.p, w.HXb.p, n, kk, nk, w.theta.p, w.part.p, nblk, w.rn2.p, s);
+    VCK(d2h(c, th.data(), w.theta.p, nk * sizeof(double)));
+    VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
+    VCK(cudaStreamSynchronize(s));
+    const int keff = std::min(k, nk);
+    int nconv = 0;
+    double rmax = 0.0;
+    for (int j = 0; j < keff; ++j) {
+      const double r = std::sqrt(std::max(rn[j], 0.0));
+      rmax = std::max(rmax, r);
+      if (r <= tol * std::max(eps23, std::fabs(th[j]))) ++nconv;
+    }
+    t_rr += msince(t0);
+    if (plevel >= 2)
+      std::fprintf(stderr, "  lanczos cycle %d m %d b %d converged %d/%d max|r| %.3e\n", cyc, m, b,
+                   nconv, keff, rmax);
+    if (nconv == keff || m >= n || exhausted) {
+      if (nconv < keff && !(m >= n || exhausted))
+        return fail(c, VHCI_E_NOT_CONVERGED, "Error: Eigenvalues did not converge.");
+      if (plevel)
+        std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
+                     (long long)n, k, b, cyc + 1, steps, t_spmm, t_orth, t_rr, msince(t_start));
+      VCK(c->X.reserve((size_t)n * kk, s));
+      VCK(cudaMemcpyAsync(c->X.p, w.Xb.p, (size_t)n * kk * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      c->ldx = kk;
+      c->nvec = nk;
+      c->x_rows = n;
+      c->E.assign(th.begin(), th.begin() + nk);
+      VCK(cudaStreamSynchronize(s));
+      w.release(s);
+      return VHCI_OK;
+    }
+    // ---- thick restart: pending block from the last expansion, then keep the Ritz block
+    t0 = now();
+    copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, n, p, s);
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.T.p + (size_t)(m - p) * ld,
+                    ld, w.Q.p, ld, &one, w.W.p, b));
+    VCK(w.S.reserve((size_t)m * p, s));
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, p, (int)n, &one, w.Q.p, ld, w.W.p, b,
+                    &zero, w.S.p, m));
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.S.p, m, w.Q.p, ld,
+                    &one, w.W.p, b));
+    copy_cols(w.Xb.p, kk, w.Q.p, ld, n, nk, s);
+    copy_cols(w.HXb.p, kk, w.HQ.p, ld, n, nk, s);
+    int p2 = 0;
+    VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + nk, ld, &p2));
+    std::vector<double> Th((size_t)ld * nk, 0.0);
+    for (int j = 0; j < nk; ++j) Th[(size_t)j * ld + j] = th[j];
+    VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
+    VCK(h2d(c, w.T.p, Th.data(), Th.size() * sizeof(double)));
+    m = nk;
+    p = p2;
+    t_rr += msince(t0);
+    if (p == 0) {  // the kept block is invariant: one more Rayleigh-Ritz finishes
+      exhausted = true;
+    }
+    if (exhausted) {
+      VCK(c->X.reserve((size_t)n * kk, s));
+      VCK(cudaMemcpyAsync(c->X.p, w.Xb.p, (size_t)n * kk * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      c->ldx = kk;
+      c->nvec = nk;
+      c->x_rows = n;
+      c->E.assign(th.begin(), th.begin() + nk);
+      VCK(cudaStreamSynchronize(s));
+      w.release(s);
+      return VHCI_OK;
+    }
+  }
+  w.release(s);
+  return fail(c, VHCI_E_NOT_CONVERGED, "Error: Eigenvalues did not converge.");
+}
+
+}  // namespace vhci

@@ -115,10 +115,12 @@ void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* va
 void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,
                     const double* theta, double* part, int nblk, double* rn2, cudaStream_t s);
 int residual_blocks(int64_t n);
-// T[i, j] = (HX[i,c_j] - theta_j X[i,c_j]) / (theta_j - d_i), c_j = cols[j]
+// Olsen-corrected diagonal-preconditioned residuals of the Ritz pairs c_j = cols[j]:
+// T[i, j] = (r_i - eps_j x_i) / (theta_j - d_i).  scratch holds correction_scratch(n, nc) doubles.
+int correction_scratch(int64_t n, int nc);
 void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
                          int64_t n, const int* cols, const double* theta, int nc, double* T,
-                         int ldt, cudaStream_t s);
+                         int ldt, double* scratch, cudaStream_t s);
 void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,
                cudaStream_t s);
 void dense_from_csr(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
