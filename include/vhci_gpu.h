@@ -154,6 +154,11 @@ vhci_status vhci_structural_nnz(vhci_ctx* c, int64_t* nnz);
  * use): the sparse product the eigensolver runs (SparseSymMatProd in the reference, Ham.cpp:349). */
 vhci_status vhci_apply_h(vhci_ctx* c, const double* X, double* Y, int b);
 
+/* Residual norms || H x_j - theta_j x_j || of k host vectors (n x k, column-major) with the
+ * current Hamiltonian: the convergence measure of the reference's eigensolver (Ham.cpp:363). */
+vhci_status vhci_residual_norms(vhci_ctx* c, const double* X, const double* theta, double* rnorm,
+                                int k);
+
 /* Lowest k eigenpairs of the current Hamiltonian (SparseDiagonalize, Ham.cpp:347-370; dense
  * eigensolve for small bases, DenseDiagonalize, :372-379).  Vectors stay on device; E (k)
  * receives the eigenvalues if not NULL. */

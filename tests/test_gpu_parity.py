@@ -146,9 +146,12 @@ def test_davidson_end_to_end_workload0(api):
     assert r["n_basis"] == g["log"]["final_basis"]
 
 
+@pytest.mark.parametrize("form", ["rg", "rows", "slots"])
 @pytest.mark.parametrize("b", [1, 5, 8, 13, 16, 31, 40, 97])
-def test_spmm_matches_csr_product(api, b):
-    """H X on the device (all column-panel widths) against the CSR product of the same matrix."""
+def test_spmm_matches_csr_product(api, b, form, monkeypatch):
+    """H X on the device (both panel kernels, all panel widths) against the CSR product of the
+    same matrix."""
+    monkeypatch.setenv("VHCI_SPMM", form)
     g = load_golden("syn_m8_sextic_pt2")
     o = O.Oracle(g["input"])
     w, C = _oracle_first_step(o)
@@ -161,6 +164,31 @@ def test_spmm_matches_csr_product(api, b):
         Y = v.apply_h(X)
     ref = H @ X
     assert np.abs(Y - ref).max() <= 1e-12 * np.abs(H).sum(axis=1).max() * np.abs(X).max()
+
+
+@pytest.mark.parametrize("k", [1, 7, 32, 45, 70])
+def test_residual_norms_match_host(api, k):
+    """Fused device residual norms ||H x - theta x|| against the same product done on the host."""
+    g = load_golden("syn_m8_sextic_pt2")
+    rng = np.random.default_rng(k)
+    with api.VHCI(g["input"]) as v:
+        H = v.h_csr()
+        X = rng.standard_normal((v.n, k))
+        th = rng.uniform(5000, 20000, k)
+        r = v.residual_norms(X, th)
+    ref = np.linalg.norm(H @ X - X * th, axis=0)
+    assert np.allclose(r, ref, rtol=1e-11, atol=0)
+
+
+def test_eigenpairs_meet_reference_tolerance(api):
+    """Eigenpairs from the sparse solver satisfy the reference's stopping rule (tol 1e-10)."""
+    g = load_golden("workload0")
+    with api.VHCI(g["input"]) as v:
+        v.hci()
+        C, E = v.vectors(v.info.nstate)
+        r = v.residual_norms(C, E)
+    eps23 = np.finfo(float).eps ** (2 / 3)
+    assert np.all(r <= 1e-10 * np.maximum(eps23, np.abs(E)) * 1.0001), (r / np.abs(E)).max()
 
 
 def test_key_layout_8bit_for_high_quanta(api):

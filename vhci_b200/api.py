@@ -27,6 +27,7 @@ EXPORTS = [
     "vhci_get_vectors", "vhci_select", "vhci_get_selected", "vhci_build_h", "vhci_get_h_csr",
     "vhci_structural_nnz", "vhci_eigs", "vhci_hci", "vhci_pt2", "vhci_write_freqs",
     "vhci_write_checkpoint", "vhci_read_checkpoint", "vhci_get_energies", "vhci_apply_h",
+    "vhci_residual_norms",
 ]
 
 
@@ -115,6 +116,7 @@ def lib():
             "vhci_structural_nnz": (ctypes.c_int, [vp, i64p]),
             "vhci_eigs": (ctypes.c_int, [vp, ctypes.c_int, dp]),
             "vhci_apply_h": (ctypes.c_int, [vp, dp, dp, ctypes.c_int]),
+            "vhci_residual_norms": (ctypes.c_int, [vp, dp, dp, dp, ctypes.c_int]),
             "vhci_hci": (ctypes.c_int, [vp, ctypes.c_char_p, vp, vp]),
             "vhci_pt2": (ctypes.c_int, [vp, ctypes.c_double, dp, i64p]),
             "vhci_write_freqs": (ctypes.c_int, [vp, ctypes.c_char_p]),
@@ -296,6 +298,15 @@ class VHCI:
         self._check(lib().vhci_apply_h(self.h, _ptr(X, ctypes.c_double), _ptr(Y, ctypes.c_double),
                                        X.shape[1]))
         return Y
+
+    def residual_norms(self, X: np.ndarray, theta: np.ndarray) -> np.ndarray:
+        X = np.asfortranarray(X, np.float64)
+        theta = np.ascontiguousarray(theta, np.float64)
+        r = np.zeros(X.shape[1])
+        self._check(lib().vhci_residual_norms(self.h, _ptr(X, ctypes.c_double),
+                                              _ptr(theta, ctypes.c_double),
+                                              _ptr(r, ctypes.c_double), X.shape[1]))
+        return r
 
     def eigs(self, k: int) -> np.ndarray:
         E = np.zeros(k)

@@ -1,6 +1,8 @@
 // Hamiltonian kernels: the connection-driven sparse build (replacing the reference's O(N^2) pair
 // loop, Ham.cpp:228-326), the SpMM that drives the eigensolver, and the Davidson vector helpers.
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 #include "conn.cuh"
 #include "ops.h"
@@ -164,6 +166,77 @@ __global__ void __launch_bounds__(256) k_spmm_panel(int64_t n, const int64_t* __
   }
 }
 
+// Row-group form of the panel product: a warp holds G = 32/BP rows, each handled by a group of BP
+// lanes that own one column each and walk the row's entries together (the entry loads are
+// broadcasts within the group and L1 hits across consecutive entries), so the inner loop has no
+// shuffles: two cached loads, one gathered load and one FMA per entry.
+template <int BP, typename VT, bool CG>
+__global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __restrict__ rowptr,
+                                                   const int32_t* __restrict__ col,
+                                                   const VT* __restrict__ val,
+                                                   const double* __restrict__ diag,
+                                                   const double* __restrict__ X, int ldx, int bp,
+                                                   double* __restrict__ Y, int ldy) {
+  constexpr int G = 32 / BP;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / BP, cc = lane % BP;
+  const bool active = cc < bp;
+  const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5) * G;
+  for (int64_t i = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * G + grp;
+       i < n; i += stride) {
+    const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
+    double acc = 0.0;
+    if (active) {
+#pragma unroll 4
+      for (int64_t e = beg; e < end; ++e) {
+        const int j = __ldg(col + e);
+        const double v = (double)__ldg(val + e);
+        const double* xp = X + (int64_t)j * ldx + cc;
+        acc = fma(v, CG ? __ldcg(xp) : __ldg(xp), acc);
+      }
+      Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
+    }
+  }
+}
+
+// Row groups with cooperative entry loads: a warp holds G = 32/BP rows; a group of BP lanes loads
+// BP consecutive entries of its row in one coalesced access, then broadcasts them one by one with
+// width-BP shuffles while each lane gathers its own column.  Per entry the L1 sees one gathered
+// BP*8-byte segment plus 2/BP of a matrix-stream access.
+template <int BP, typename VT>
+__global__ void __launch_bounds__(256) k_spmm_rg(int64_t n, const int64_t* __restrict__ rowptr,
+                                                 const int32_t* __restrict__ col,
+                                                 const VT* __restrict__ val,
+                                                 const double* __restrict__ diag,
+                                                 const double* __restrict__ X, int ldx, int bp,
+                                                 double* __restrict__ Y, int ldy) {
+  constexpr int G = 32 / BP;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / BP, cc = lane % BP;
+  const unsigned gmask = (BP == 32) ? 0xffffffffu : (((1u << BP) - 1u) << (grp * BP));
+  const bool active = cc < bp;
+  const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5) * G;
+  for (int64_t i = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * G + grp;
+       i < n; i += stride) {
+    const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
+    double acc = 0.0;
+    for (int64_t e0 = beg; e0 < end; e0 += BP) {
+      const int64_t e = e0 + cc;
+      int jj = 0;
+      double vv = 0.0;
+      if (e < end) { jj = __ldcs(col + e); vv = (double)__ldcs(val + e); }
+      const int m = (int)(end - e0 < BP ? end - e0 : BP);
+#pragma unroll 8
+      for (int t = 0; t < m; ++t) {
+        const int j = __shfl_sync(gmask, jj, t, BP);
+        const double v = __shfl_sync(gmask, vv, t, BP);
+        if (active) acc = fma(v, __ldg(X + (int64_t)j * ldx + cc), acc);
+      }
+    }
+    if (active) Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
+  }
+}
+
 // L2 budget for one panel of gathered vector columns (bytes); B200 has 126 MB of L2.
 constexpr double kSpmmL2Budget = 64e6;
 
@@ -172,19 +245,44 @@ void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const V
                    const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
                    cudaStream_t s) {
   const int g = grid_for(n * 32, 256, 148 * 16);
-  // L2 holds whole 128-byte lines: a panel of BP columns occupies n * max(128, 8 BP) bytes
-  const double lines = (double)n * 128.0;
-  if (lines * ((b + 15) / 16) > kSpmmL2Budget || b <= 16) {
-    // column panels: 32 columns when two lines per row fit the budget, else 16 (one line per row;
-    // 8 only for blocks of at most 8 columns)
-    int BP = (lines * 2 <= kSpmmL2Budget) ? 32 : 16;
-    if (b <= 8) BP = 8;
+  // L2 holds whole 128-byte lines: a strided panel of BP columns occupies n * max(128, 8 BP)
+  // bytes, a compact one (ldx == b) n * 8 b bytes
+  const double rowbytes = (ldx == b) ? 8.0 * b : 128.0 * ((b + 15) / 16);
+  if ((double)n * rowbytes > kSpmmL2Budget || b <= 32) {
+    int BP = 32;
+    if (b <= 4) BP = 4;
+    else if (b <= 8) BP = 8;
     else if (b <= 16) BP = 16;
+    else if (ldx != b && (double)n * 256.0 > kSpmmL2Budget) BP = 16;
+    const char* fe = std::getenv("VHCI_SPMM");
+    const std::string form = fe ? fe : "";
+    const bool slots = form == "slots";
     for (int c0 = 0; c0 < b; c0 += BP) {
       const int bp = std::min(BP, b - c0);
-      if (BP == 32) { note_launch(); k_spmm_panel<32, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-      else if (BP == 16) { note_launch(); k_spmm_panel<16, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-      else { note_launch(); k_spmm_panel<8, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      if (slots) {
+        if (BP == 4) BP = 8;
+        if (BP == 32) { note_launch(); k_spmm_panel<32, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else if (BP == 16) { note_launch(); k_spmm_panel<16, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else { note_launch(); k_spmm_panel<8, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      } else if (form == "rg") {
+        const int gr = grid_for(n * BP, 256, 148 * 16);
+        if (BP == 32) { note_launch(); k_spmm_rg<32, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else if (BP == 16) { note_launch(); k_spmm_rg<16, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else if (BP == 8) { note_launch(); k_spmm_rg<8, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else { note_launch(); k_spmm_rg<4, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      } else if (form == "rows_cg") {
+        if (BP == 4) BP = 8;
+        const int gr = grid_for(n * BP, 256, 148 * 16);
+        if (BP == 32) { note_launch(); k_spmm_rows<32, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else if (BP == 16) { note_launch(); k_spmm_rows<16, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else { note_launch(); k_spmm_rows<8, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      } else {
+        if (BP == 4) BP = 8;
+        const int gr = grid_for(n * BP, 256, 148 * 16);
+        if (BP == 32) { note_launch(); k_spmm_rows<32, VT, false><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else if (BP == 16) { note_launch(); k_spmm_rows<16, VT, false><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        else { note_launch(); k_spmm_rows<8, VT, false><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+      }
     }
     return;
   }

@@ -1,8 +1,8 @@
 // Block thick-restart Lanczos for the lowest eigenpairs of the sparse Hamiltonian — the same
 // method family as the reference's eigensolver (implicitly restarted Lanczos, SparseDiagonalize,
 // Ham.cpp:347-370), organised for the GPU:
-//   * blocks of b = 16 or 32 vectors (sized so the block's 128-byte L2 lines stay resident), so the
-//     SpMM streams the matrix from HBM once per block while the per-entry gathers hit L2;
+//   * blocks of b = 16 or 32 vectors; the SpMM gathers from a compact n x b copy of the block and
+//     streams the matrix from HBM once per block;
 //   * full reorthogonalisation (classical Gram-Schmidt, two passes) with FP64 GEMMs, and the
 //     projected matrix T = Q^T H Q formed explicitly from the stored H Q blocks;
 //   * Rayleigh-Ritz (cuSOLVER syevd on T) only when the subspace is full; the kk = k + guard
@@ -77,10 +77,11 @@ void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std::vecto
 }
 
 struct LWork {
-  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2;
+  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc;
   void release(cudaStream_t s) {
     Q.release(s); HQ.release(s); T.release(s); Yw.release(s); theta.release(s); Xb.release(s);
     HXb.release(s); W.release(s); S.release(s); M.release(s); part.release(s); rn2.release(s);
+    Xc.release(s);
   }
 };
 
@@ -142,13 +143,17 @@ int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb
   return VHCI_OK;
 }
 
-int apply_h_l(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
+// Y = H X for a block: X is first copied to a compact n x b buffer so the SpMM gathers from a
+// small, L2-resident array instead of rows of the wide basis.
+int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y, int ldy) {
   cudaEvent_t e0, e1;
   VCK(cudaEventCreate(&e0));
   VCK(cudaEventCreate(&e1));
+  VCK(w.Xc.reserve((size_t)c->n * b, c->st));
   VCK(cudaEventRecord(e0, c->st));
+  copy_cols(X, ldx, w.Xc.p, b, c->n, b, c->st);
   spmm(c->n, c->rowptr.p, c->col.p, c->o.precision == 1 ? nullptr : c->val.p,
-       c->o.precision == 1 ? c->valf.p : nullptr, c->diag.p, X, ldx, b, Y, ldy, c->st);
+       c->o.precision == 1 ? c->valf.p : nullptr, c->diag.p, w.Xc.p, b, b, Y, ldy, c->st);
   VCK(cudaEventRecord(e1, c->st));
   VCK(cudaEventSynchronize(e1));
   VCK(cudaGetLastError());
@@ -166,9 +171,11 @@ int apply_h_l(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) 
 
 }  // namespace
 
-// Block size for a basis of n states: 32 when the block's L2 lines (two 128-byte lines per row)
-// fit 64 MB, else 16 (one line per row, the narrowest block that uses whole lines).
-int lanczos_block(int64_t n) { return (double)n * 256.0 <= 64e6 ? 32 : 16; }
+// Block size for a basis of n states.  The SpMM's cost per vector column falls with the block
+// width (the per-entry matrix loads are shared by more columns) and so does the reorthogonalisation
+// cost per column (one pass over the basis serves the whole block); wide blocks need somewhat more
+// products in total.  Measured on B200: 32 columns up to 150k states, 16 above.
+int lanczos_block(int64_t n) { return n <= 150000 ? 32 : 16; }
 
 int block_lanczos(vhci_ctx* c, int k) {
   const int64_t n = c->n;
@@ -247,7 +254,7 @@ int block_lanczos(vhci_ctx* c, int k) {
     bool exhausted = (p == 0);
     while (p > 0) {
       auto t0 = now();
-      VTRY(apply_h_l(c, w.Q.p + m, ld, p, w.HQ.p + m, ld));
+      VTRY(apply_h_l(c, w, w.Q.p + m, ld, p, w.HQ.p + m, ld));
       t_spmm += msince(t0);
       t0 = now();
       ++steps;
