@@ -158,6 +158,22 @@ vhci_status vhci_apply_h(vhci_ctx* c, const double* X, double* Y, int b);
  * current Hamiltonian: the convergence measure of the reference's eigensolver (Ham.cpp:363). */
 vhci_status vhci_residual_norms(vhci_ctx* c, const double* X, const double* theta, double* rnorm,
                                 int k);
+/* The same residual norms for callers that cannot allocate device memory when they need them (a
+ * serving process whose device memory belongs to its own pool, or code that must avoid the implicit
+ * device-wide synchronisation of cudaMalloc/cudaFree).  No counterpart in the reference.
+ * Inputs and outputs are DEVICE pointers on the context's device: X_dev is n x k row-major
+ * (ld = k), theta_dev has k values, rnorm_dev receives k values; results are ready when the call
+ * returns.  The call allocates nothing: its scratch is a fixed array of 296 x 256 doubles (606 KB)
+ * in the library's device memory, which every device that loads the library keeps until the
+ * process exits.  Limits and rules:
+ *  - 1 <= k <= 256, else VHCI_E_INPUT;
+ *  - the Hamiltonian must already be built (vhci_build_h), else VHCI_E_STATE;
+ *  - the first call on a device looks up the scratch array's device address (and may load the
+ *    library's device code); make that first call before any stream capture;
+ *  - all calls share the one array: calls whose work overlaps on the GPU (from several threads or
+ *    contexts on one device) race and must be serialised by the caller. */
+vhci_status vhci_residual_norms_noalloc(vhci_ctx* c, const double* X_dev, const double* theta_dev,
+                                        double* rnorm_dev, int k);
 
 /* Lowest k eigenpairs of the current Hamiltonian (SparseDiagonalize, Ham.cpp:347-370; dense
  * eigensolve for small bases, DenseDiagonalize, :372-379).  Vectors stay on device; E (k)

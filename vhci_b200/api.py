@@ -27,7 +27,7 @@ EXPORTS = [
     "vhci_get_vectors", "vhci_select", "vhci_get_selected", "vhci_build_h", "vhci_get_h_csr",
     "vhci_structural_nnz", "vhci_eigs", "vhci_hci", "vhci_pt2", "vhci_write_freqs",
     "vhci_write_checkpoint", "vhci_read_checkpoint", "vhci_get_energies", "vhci_apply_h",
-    "vhci_residual_norms",
+    "vhci_residual_norms", "vhci_residual_norms_noalloc",
 ]
 
 
@@ -117,6 +117,7 @@ def lib():
             "vhci_eigs": (ctypes.c_int, [vp, ctypes.c_int, dp]),
             "vhci_apply_h": (ctypes.c_int, [vp, dp, dp, ctypes.c_int]),
             "vhci_residual_norms": (ctypes.c_int, [vp, dp, dp, dp, ctypes.c_int]),
+            "vhci_residual_norms_noalloc": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
             "vhci_hci": (ctypes.c_int, [vp, ctypes.c_char_p, vp, vp]),
             "vhci_pt2": (ctypes.c_int, [vp, ctypes.c_double, dp, i64p]),
             "vhci_write_freqs": (ctypes.c_int, [vp, ctypes.c_char_p]),
@@ -307,6 +308,13 @@ class VHCI:
                                               _ptr(theta, ctypes.c_double),
                                               _ptr(r, ctypes.c_double), X.shape[1]))
         return r
+
+    def residual_norms_noalloc(self, x_dev: int, theta_dev: int, rnorm_dev: int, k: int) -> None:
+        """Residual norms over caller-owned DEVICE buffers (addresses as integers): X n x k
+        row-major, theta k, rnorm k.  Allocates nothing (see include/vhci_gpu.h)."""
+        self._check(lib().vhci_residual_norms_noalloc(self.h, ctypes.c_void_p(x_dev),
+                                                      ctypes.c_void_p(theta_dev),
+                                                      ctypes.c_void_p(rnorm_dev), k))
 
     def eigs(self, k: int) -> np.ndarray:
         E = np.zeros(k)

@@ -4,6 +4,7 @@
 // (the SpMM of k_ham.cu), subtract theta x_i, square, and add into per-block partial sums kept in
 // scratch memory; a second kernel sums the partials in a fixed order.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "internal.h"
@@ -121,5 +122,59 @@ extern "C" vhci_status vhci_residual_norms(vhci_ctx* c, const double* X, const d
   dth.release(c->st);
   part.release(c->st);
   dr.release(c->st);
+  return VHCI_OK;
+}
+
+// ---- residual norms without allocation ------------------------------------------------------
+//
+// Some callers cannot allocate device memory at the point where they need this check: a serving
+// process whose device memory is owned by its own pool, or code that must not trigger the implicit
+// device-wide synchronisation of cudaMalloc/cudaFree in the middle of its work.  For them the
+// per-block partial sums live in a fixed array in the library's device memory instead of a buffer
+// allocated per call.  The array holds kResidBlocks x kNoAllocMaxCols doubles (606 KB) and stays
+// resident on every device that loads the library until the process exits.
+
+namespace {
+
+constexpr int kNoAllocMaxCols = 256;
+__device__ __align__(256) double g_resid_scratch[kResidBlocks * kNoAllocMaxCols];
+
+std::mutex g_scratch_mu;
+double* g_scratch_dev[128] = {nullptr};  // device address of g_resid_scratch per device ordinal
+
+}  // namespace
+
+extern "C" vhci_status vhci_residual_norms_noalloc(vhci_ctx* c, const double* X_dev,
+                                                   const double* theta_dev, double* rnorm_dev,
+                                                   int k) {
+  if (!c || !X_dev || !theta_dev || !rnorm_dev) return VHCI_E_INPUT;
+  if (k <= 0 || k > kNoAllocMaxCols)
+    return fail(c, VHCI_E_INPUT,
+                "vhci_residual_norms_noalloc: k must be between 1 and 256 (the size of its "
+                "fixed scratch array)");
+  if (!c->h_valid)
+    return fail(c, VHCI_E_STATE,
+                "vhci_residual_norms_noalloc: the Hamiltonian is not built; call vhci_build_h "
+                "first (building it allocates, this call does not)");
+  const int dev = c->o.device;
+  if (dev < 0 || dev >= 128) return fail(c, VHCI_E_CUDA, "device ordinal out of range");
+  VCK(cudaSetDevice(dev));
+  double* scratch = nullptr;
+  {
+    // set-up, once per device with that device current: host code only has a host-side stand-in
+    // for the array's name, so the device address is looked up and kept
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_dev[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_resid_scratch);
+      if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetSymbolAddress(g_resid_scratch)");
+      g_scratch_dev[dev] = static_cast<double*>(p);
+    }
+    scratch = g_scratch_dev[dev];
+  }
+  // every block writes all of its partial sums, so nothing left from an earlier call is read
+  residual_norms_fused(c, X_dev, k, theta_dev, scratch, rnorm_dev);
+  VCK(cudaGetLastError());
+  VCK(cudaStreamSynchronize(c->st));
   return VHCI_OK;
 }
