@@ -42,6 +42,10 @@ WORKLOAD_DESC = ("VHCI+PT2, synthetic PES Nm=15 (cubic p=0.5 +-10^U(0,2.5), quar
                  "+-10^U(-1,1.5)), HCI_Eps=0.5, Nstate=200, PT2_Eps=0.01, Max_quanta=2")
 # Basis size after each heat-bath iteration and |P| of the workload-1 solve (FP64 path).
 WORKLOAD_COUNTS = {"sizes": [38934, 215006, 336950, 372333, 380418], "n_pert": 6583465}
+# DRAM bytes per k_spmm_rows launch, averaged over the 1070 launches of one workload-1 solve, from
+# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of
+# `vhci_b200/bin/vhci -n 1 -i <workload-1 input> -o <out>` on B200.
+NCU_SPMM_TRAFFIC_PER_LAUNCH = 2.896e9
 
 
 def _dist():
@@ -264,9 +268,11 @@ def run_ours(args):
     spmm_gbs = st["spmm_bytes"] / (st["ms_spmm"] / 1e3) / 1e9 if st["ms_spmm"] else None
     en_gbs = (st["pt2_reduce_bytes"] / (st["ms_pt2_reduce"] / 1e3) / 1e9
               if st["ms_pt2_reduce"] else None)
-    roof = {"bound": "hbm", "kernel": "k_spmm (eigensolver H*X)", "achieved": spmm_gbs,
+    alg_per_launch = st["spmm_bytes"] / st["spmm_calls"] if st["spmm_calls"] else None
+    roof = {"bound": "hbm", "kernel": "k_spmm_rows (eigensolver H*X)", "achieved": spmm_gbs,
             "peak": hbm, "unit": "GB/s", "frac": (spmm_gbs / hbm) if spmm_gbs else None,
-            "traffic": args.traffic, "peak_kind": peak_kind,
+            "traffic": args.traffic if args.traffic else NCU_SPMM_TRAFFIC_PER_LAUNCH,
+            "algorithmic_bytes_per_launch": alg_per_launch, "peak_kind": peak_kind,
             "other": {"k_pt2_en GB/s": en_gbs}}
 
     line = {
@@ -302,6 +308,33 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_spmm_sweep(args):
+    """Solve the workload, then time the sparse product H X on the final basis for several block
+    widths and both panel kernels (CUDA events around the product only)."""
+    import numpy as np
+    from vhci_b200 import api
+    td = tempfile.mkdtemp(prefix="vhci_sweep_")
+    path = os.path.join(td, "workload.inp")
+    write_workload(path)
+    with api.VHCI(path) as v:
+        v.hci()
+        rng = np.random.default_rng(0)
+        print(json.dumps({"n": v.n, "nnz": int(v.info.h_nnz)}), flush=True)
+        for b in (4, 8, 16, 32):
+            X = rng.standard_normal((v.n, b))
+            for form in ("rows", "slots"):
+                os.environ["VHCI_SPMM"] = form
+                v.apply_h(X)
+                s0 = v.stats()
+                for _ in range(8):
+                    v.apply_h(X)
+                s1 = v.stats()
+                ms = (s1["ms_spmm"] - s0["ms_spmm"]) / 8
+                print(json.dumps({"b": b, "kernel": form, "ms": round(ms, 3),
+                                  "ms_per_column": round(ms / b, 4)}), flush=True)
+        os.environ.pop("VHCI_SPMM", None)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,7 +346,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per SpMM launch, if captured")
+    ap.add_argument("--spmm-sweep", action="store_true",
+                    help="time the sparse product on the workload's final basis and exit")
     args = ap.parse_args()
+    if args.spmm_sweep:
+        run_spmm_sweep(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -187,13 +187,40 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
     const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
     double acc = 0.0;
     if (active) {
-#pragma unroll 4
-      for (int64_t e = beg; e < end; ++e) {
-        const int j = __ldg(col + e);
-        const double v = (double)__ldg(val + e);
+      auto gx = [&](int j) {
         const double* xp = X + (int64_t)j * ldx + cc;
-        acc = fma(v, CG ? __ldcg(xp) : __ldg(xp), acc);
+        return CG ? __ldcg(xp) : __ldg(xp);
+      };
+      int64_t e = beg;
+      if constexpr (sizeof(VT) == 8) {
+        // entries four at a time: one 16-byte column load and two 16-byte value loads, each a
+        // broadcast within the group, after a scalar prologue to 4-entry alignment
+        for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
+        for (; e + 4 <= end; e += 4) {
+          const int4 j4 = __ldg(reinterpret_cast<const int4*>(col + e));
+          const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + e));
+          const double2 v23 = __ldg(reinterpret_cast<const double2*>(val + e + 2));
+          const double x0 = gx(j4.x), x1 = gx(j4.y), x2 = gx(j4.z), x3 = gx(j4.w);
+          acc = fma((double)v01.x, x0, acc);
+          acc = fma((double)v01.y, x1, acc);
+          acc = fma((double)v23.x, x2, acc);
+          acc = fma((double)v23.y, x3, acc);
+        }
+      } else {
+        // FP32 values: one 16-byte column load and one 16-byte value load per four entries
+        for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
+        for (; e + 4 <= end; e += 4) {
+          const int4 j4 = __ldg(reinterpret_cast<const int4*>(col + e));
+          const float4 v4 = __ldg(reinterpret_cast<const float4*>(val + e));
+          const double x0 = gx(j4.x), x1 = gx(j4.y), x2 = gx(j4.z), x3 = gx(j4.w);
+          acc = fma((double)v4.x, x0, acc);
+          acc = fma((double)v4.y, x1, acc);
+          acc = fma((double)v4.z, x2, acc);
+          acc = fma((double)v4.w, x3, acc);
+        }
       }
+#pragma unroll 4
+      for (; e < end; ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
       Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
     }
   }
