@@ -1,7 +1,7 @@
 // Block thick-restart Lanczos for the lowest eigenpairs of the sparse Hamiltonian — the same
 // method family as the reference's eigensolver (implicitly restarted Lanczos, SparseDiagonalize,
 // Ham.cpp:347-370), organised for the GPU:
-//   * blocks of b = 16 or 32 vectors; the SpMM gathers from a compact n x b copy of the block and
+//   * blocks of b = 16 vectors; the SpMM gathers from a compact n x b copy of the block and
 //     streams the matrix from HBM once per block;
 //   * full reorthogonalisation (classical Gram-Schmidt, two passes) with FP64 GEMMs, and the
 //     projected matrix T = Q^T H Q formed explicitly from the stored H Q blocks;
@@ -171,11 +171,16 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
 
 }  // namespace
 
-// Block size for a basis of n states.  The SpMM's cost per vector column falls with the block
-// width (the per-entry matrix loads are shared by more columns) and so does the reorthogonalisation
-// cost per column (one pass over the basis serves the whole block); wide blocks need somewhat more
-// products in total.  Measured on B200: 32 columns up to 150k states, 16 above.
-int lanczos_block(int64_t n) { return n <= 150000 ? 32 : 16; }
+// Block size.  The SpMM's cost per vector column falls with the block width (the per-entry matrix
+// loads are shared by more columns) and so does the reorthogonalisation cost per column (one pass
+// over the basis serves the whole block), while wider blocks need more products in total.  Measured
+// on B200 over the workload-1 solve (39k..380k states, k = 200): 16 is best at every size
+// (VHCI_LANCZOS_BLOCK overrides it).
+int lanczos_block(int64_t n) {
+  (void)n;
+  if (const char* e = std::getenv("VHCI_LANCZOS_BLOCK")) return std::max(4, std::min(32, std::atoi(e)));
+  return 16;
+}
 
 int block_lanczos(vhci_ctx* c, int k) {
   const int64_t n = c->n;
@@ -183,7 +188,10 @@ int block_lanczos(vhci_ctx* c, int k) {
   const int guard = std::max(8, k / 10);
   const int kk = (int)std::min<int64_t>(n, k + guard);
   const int b = lanczos_block(n);
-  const int mmax = (int)std::min<int64_t>(n, (int64_t)3 * kk + 2 * b);
+  // subspace size: 3 kk + 2 b by default (VHCI_LANCZOS_SPAN overrides the factor 3)
+  int span = 3;
+  if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) span = std::max(2, std::min(8, std::atoi(e)));
+  const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
   const double one = 1.0, zero = 0.0, mone = -1.0;
