@@ -335,6 +335,101 @@ def run_spmm_sweep(args):
         os.environ.pop("VHCI_SPMM", None)
 
 
+def _write_serving_request(r, path):
+    from vhci_b200 import pes as P
+    spec, run = P.serving_request(r)
+    P.write_input(path, spec, run)
+    return {"nm": len(spec.freqs), "nstate": run.nstate, "eps1": run.eps1}
+
+
+def _pct(x, p):
+    import numpy as np
+    return float(np.percentile(np.asarray(x), p)) if len(x) else None
+
+
+def run_serving(args):
+    """Serving stream: R requests (fresh admissible PES each, Nm 6..24, Nstate 10..100, eps1
+    log-uniform in [0.3, 3], PT2 with eps2 = 0.1 eps1) with Poisson arrivals, under per-request size
+    limits (basis and perturber space; a request past them is rejected with E_LIMIT by both paths).
+    The one-at-a-time path is the same server with one slot and every request queued at t = 0: its
+    service times s_i give its latencies under the Poisson arrivals (c_i = max(a_i, c_{i-1}) + s_i).
+    The server (continuous batching over `slots` concurrent contexts) then replays the arrivals in
+    real time.  The arrival rate defaults to 1.5x the one-at-a-time throughput."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    import numpy as np
+    td = tempfile.mkdtemp(prefix="vhci_serve_")
+    paths = [os.path.join(td, f"req{r:03d}.inp") for r in range(args.requests)]
+    # request generation (PES draws + admissibility screen) on host processes, before any GPU call
+    with ProcessPoolExecutor(max_workers=min(32, os.cpu_count() or 1),
+                             mp_context=mp.get_context("spawn")) as ex:
+        meta = list(ex.map(_write_serving_request, range(args.requests), paths))
+    from vhci_b200 import api
+    lim = {"max_basis": args.max_basis, "max_pert": args.max_pert}
+    small = min(range(len(paths)), key=lambda i: meta[i]["nm"])
+    api.serve([(paths[small], 0.0)], slots=1, **lim)      # warm-up: module load, handles, pool
+    _, seq = api.serve([(p, 0.0) for p in paths], slots=1, **lim)
+    service = [r["t_done"] - r["t_admit"] for r in seq]
+    if args.verbose_requests:
+        for i, (m, r, s) in enumerate(zip(meta, seq, service)):
+            print(json.dumps({"request": i, **m, "status": r["status"], "n_basis": r["n_basis"],
+                              "n_pert": r["n_pert"], "service_s": round(s, 4),
+                              "message": r["message"]}), file=sys.stderr, flush=True)
+    ok = [r["status"] == 0 for r in seq]
+    seq_tput = sum(ok) / sum(service)
+    rate = args.rate if args.rate else 1.5 * len(paths) / sum(service)
+    rng = np.random.default_rng(12345)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(paths)))
+    arrivals -= arrivals[0]
+    c, seq_lat = 0.0, []
+    for a, s, g in zip(arrivals, service, ok):
+        c = max(a, c) + s
+        if g:
+            seq_lat.append(c - a)
+    seq_wall = c
+    summ, res = api.serve(list(zip(paths, arrivals)), slots=args.slots, reserve_bytes=8e9, **lim)
+    lat = [r["t_done"] - r["arrival"] for r in res if r["status"] == 0]
+    worst, mismatched = 0.0, 0
+    for a, r in zip(seq, res):
+        if a["status"] != r["status"]:
+            mismatched += 1
+        elif r["status"] == 0:
+            if (r["n_basis"], r["n_pert"]) != (a["n_basis"], a["n_pert"]):
+                mismatched += 1
+            worst = max(worst, float(np.abs(r["E"] - a["E"]).max()))
+    done = [r for r in seq if r["status"] == 0]
+    line = {
+        "metric": "serving_throughput", "value": round(summ["completed"] / summ["wall_s"], 4),
+        "unit": "req/s", "higher_is_better": True, "n_gpus": 1, "requests": len(paths),
+        "completed": summ["completed"],
+        "rejected_limit": sum(r["status"] == api.E_LIMIT for r in res),
+        "failed_other": sum(r["status"] not in (0, api.E_LIMIT) for r in res),
+        "slots": args.slots, "arrival_rate": round(rate, 4),
+        "p50_s": round(_pct(lat, 50), 4) if lat else None,
+        "p99_s": round(_pct(lat, 99), 4) if lat else None,
+        "wall_s": round(summ["wall_s"], 3), "peak_in_flight": summ["peak_in_flight"],
+        "oom_retries": int(sum(r["retries"] for r in res)),
+        "mix_vs_alone": {"max_abs_dE_cm1": worst, "mismatched_requests": mismatched},
+        "one_at_a_time": {"value": round(seq_tput, 4), "unit": "req/s",
+                          "service_s_total": round(sum(service), 3),
+                          "p50_s": round(_pct(seq_lat, 50), 4) if seq_lat else None,
+                          "p99_s": round(_pct(seq_lat, 99), 4) if seq_lat else None,
+                          "wall_s_under_arrivals": round(seq_wall, 3)},
+        "sizes": {"nm_max": max(m["nm"] for m in meta),
+                  "n_basis_p50": int(_pct([r["n_basis"] for r in done], 50)) if done else 0,
+                  "n_basis_max": int(max([r["n_basis"] for r in done] or [0])),
+                  "n_pert_max": int(max([r["n_pert"] for r in done] or [0])),
+                  "service_s_p50": round(_pct(service, 50), 4),
+                  "service_s_max": round(max(service), 4)},
+        "data": "synthetic", "dtype": "f64",
+        "config": {"workload": "serving stream, Poisson arrivals, Nm 6..24, Nstate 10..100, "
+                               "eps1 log-uniform [0.3,3], PT2 eps2=0.1*eps1",
+                   "max_basis": args.max_basis, "max_pert": args.max_pert},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -348,9 +443,20 @@ def main():
                     help="ncu dram bytes per SpMM launch, if captured")
     ap.add_argument("--spmm-sweep", action="store_true",
                     help="time the sparse product on the workload's final basis and exit")
+    ap.add_argument("--serving", action="store_true",
+                    help="run the request-serving stream (one GPU) and exit")
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--rate", type=float, default=None, help="Poisson arrival rate, req/s")
+    ap.add_argument("--max-basis", type=int, default=500_000)
+    ap.add_argument("--max-pert", type=int, default=100_000_000)
+    ap.add_argument("--verbose-requests", action="store_true")
     args = ap.parse_args()
     if args.spmm_sweep:
         run_spmm_sweep(args)
+        return
+    if args.serving:
+        run_serving(args)
         return
     if args.impl == "reference":
         run_reference(args)

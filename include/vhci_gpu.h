@@ -36,7 +36,8 @@ enum {
   VHCI_E_NOT_CONVERGED = 5, /* eigensolver hit its iteration limit (reference: Ham.cpp:367-368)  */
   VHCI_E_CUDA = 6,          /* CUDA runtime / library failure                                    */
   VHCI_E_STATE = 7,         /* call made in the wrong state (e.g. no vectors yet)                */
-  VHCI_E_NEG_ZPE = 8        /* zero-point energy < 0 (reference: VHCI.cpp:122-137)               */
+  VHCI_E_NEG_ZPE = 8,       /* zero-point energy < 0 (reference: VHCI.cpp:122-137)               */
+  VHCI_E_LIMIT = 9          /* the basis or perturber space would exceed max_basis / max_pert    */
 };
 
 typedef struct vhci_ctx vhci_ctx;
@@ -54,6 +55,10 @@ typedef struct {
   int64_t pt2_chunk;   /* max perturber-Hamiltonian entries held at once (0 = automatic)        */
   int structural_nnz;  /* 1: also count the reference's structural Hamiltonian entries for the
                           "% sparse" log line (Ham.cpp:341-342); costs one extra pass           */
+  int64_t max_basis;   /* 0 = no limit; else a heat-bath iteration whose selection would grow the
+                          basis past this fails with VHCI_E_LIMIT before building H             */
+  int64_t max_pert;    /* 0 = no limit; else PT2 fails with VHCI_E_LIMIT when the screened
+                          perturber space is larger, before the perturber Hamiltonian is built  */
 } vhci_opts;
 
 /* Problem description in memory (the content of a reference input file, Input_Reader.cpp). */
@@ -197,6 +202,45 @@ vhci_status vhci_read_checkpoint(vhci_ctx* c, const char* path);
 
 /* Eigenvalues currently held (n <= k). */
 vhci_status vhci_get_energies(const vhci_ctx* c, double* E, int k, int* n);
+
+/* ---- request server (continuous batching of independent solves on one GPU) ----------------
+ * No counterpart in the reference program, which solves one input per process.  Each request is
+ * a reference-format input file (or an in-memory problem) with an arrival time in seconds after
+ * the call starts.  A request is admitted into one of `slots` workers once it has arrived, a slot
+ * is free and the device's free memory is at least `reserve_bytes` (or nothing else runs); every
+ * admitted request has its own context and CUDA stream, so concurrent requests overlap on the GPU.
+ * A request that runs out of device memory is retried after another request finishes.
+ * Energies of request i go to energies[i * max_states ...] (first n_energies values). */
+typedef struct {
+  const char* input_path;          /* input file, or NULL to use `problem`                      */
+  const vhci_problem* problem;
+  double arrival_s;                /* arrival time after the start of vhci_serve                */
+} vhci_request;
+
+typedef struct {
+  int device;
+  int slots;                       /* concurrent requests (default 8)                           */
+  double reserve_bytes;            /* free device memory required to admit (default 8e9)        */
+  int max_states;                  /* energies stored per request (default 256)                 */
+  int64_t max_basis, max_pert;     /* per-request size limits, as in vhci_opts (default 0: none)  */
+} vhci_serve_opts;
+
+typedef struct {
+  int status;                      /* vhci_status of the request                                */
+  int worker, retries, n_energies;
+  int64_t n_basis, n_pert;
+  double t_admit, t_done;          /* seconds after the start of vhci_serve                     */
+  char message[160];
+} vhci_result;
+
+typedef struct {
+  double wall_s;
+  int completed, failed, peak_in_flight;
+} vhci_serve_summary;
+
+void vhci_default_serve_opts(vhci_serve_opts* so);
+vhci_status vhci_serve(const vhci_request* reqs, int nreq, const vhci_serve_opts* so,
+                       vhci_result* results, double* energies, vhci_serve_summary* summary);
 
 #ifdef __cplusplus
 }

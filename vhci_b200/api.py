@@ -15,9 +15,11 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libvhci_gpu.so")
 
-OK, E_INPUT, E_OOM, E_TABLE_FULL, E_KEY_OVERFLOW, E_NOT_CONVERGED, E_CUDA, E_STATE, E_NEG_ZPE = range(9)
+(OK, E_INPUT, E_OOM, E_TABLE_FULL, E_KEY_OVERFLOW, E_NOT_CONVERGED, E_CUDA, E_STATE, E_NEG_ZPE,
+ E_LIMIT) = range(10)
 _NAMES = {0: "OK", 1: "E_INPUT", 2: "E_OOM", 3: "E_TABLE_FULL", 4: "E_KEY_OVERFLOW",
-          5: "E_NOT_CONVERGED", 6: "E_CUDA", 7: "E_STATE", 8: "E_NEG_ZPE"}
+          5: "E_NOT_CONVERGED", 6: "E_CUDA", 7: "E_STATE", 8: "E_NEG_ZPE",
+          9: "E_LIMIT"}
 
 # Every symbol declared in include/vhci_gpu.h.
 EXPORTS = [
@@ -27,7 +29,7 @@ EXPORTS = [
     "vhci_get_vectors", "vhci_select", "vhci_get_selected", "vhci_build_h", "vhci_get_h_csr",
     "vhci_structural_nnz", "vhci_eigs", "vhci_hci", "vhci_pt2", "vhci_write_freqs",
     "vhci_write_checkpoint", "vhci_read_checkpoint", "vhci_get_energies", "vhci_apply_h",
-    "vhci_residual_norms", "vhci_residual_norms_noalloc",
+    "vhci_residual_norms", "vhci_residual_norms_noalloc", "vhci_default_serve_opts", "vhci_serve",
 ]
 
 
@@ -41,7 +43,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("eig_tol", ctypes.c_double),
                 ("eig_maxit", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("host_threads", ctypes.c_int), ("pt2_chunk", ctypes.c_int64),
-                ("structural_nnz", ctypes.c_int)]
+                ("structural_nnz", ctypes.c_int), ("max_basis", ctypes.c_int64),
+                ("max_pert", ctypes.c_int64)]
 
 
 class Problem(ctypes.Structure):
@@ -60,6 +63,29 @@ class Info(ctypes.Structure):
                 ("n_basis", ctypes.c_int64), ("n_fc", ctypes.c_int64), ("n_hb", ctypes.c_int64),
                 ("n_groups", ctypes.c_int64), ("n_vectors", ctypes.c_int64),
                 ("h_nnz", ctypes.c_int64)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("input_path", ctypes.c_char_p), ("problem", ctypes.c_void_p),
+                ("arrival_s", ctypes.c_double)]
+
+
+class ServeOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int),
+                ("reserve_bytes", ctypes.c_double), ("max_states", ctypes.c_int),
+                ("max_basis", ctypes.c_int64), ("max_pert", ctypes.c_int64)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("worker", ctypes.c_int), ("retries", ctypes.c_int),
+                ("n_energies", ctypes.c_int), ("n_basis", ctypes.c_int64),
+                ("n_pert", ctypes.c_int64), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("message", ctypes.c_char * 160)]
+
+
+class ServeSummary(ctypes.Structure):
+    _fields_ = [("wall_s", ctypes.c_double), ("completed", ctypes.c_int),
+                ("failed", ctypes.c_int), ("peak_in_flight", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -116,6 +142,10 @@ def lib():
             "vhci_structural_nnz": (ctypes.c_int, [vp, i64p]),
             "vhci_eigs": (ctypes.c_int, [vp, ctypes.c_int, dp]),
             "vhci_apply_h": (ctypes.c_int, [vp, dp, dp, ctypes.c_int]),
+            "vhci_default_serve_opts": (None, [ctypes.POINTER(ServeOpts)]),
+            "vhci_serve": (ctypes.c_int, [ctypes.POINTER(Request), ctypes.c_int,
+                                          ctypes.POINTER(ServeOpts), ctypes.POINTER(Result), dp,
+                                          ctypes.POINTER(ServeSummary)]),
             "vhci_residual_norms": (ctypes.c_int, [vp, dp, dp, dp, ctypes.c_int]),
             "vhci_residual_norms_noalloc": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
             "vhci_hci": (ctypes.c_int, [vp, ctypes.c_char_p, vp, vp]),
@@ -361,6 +391,43 @@ def _problem_struct(p: dict):
                 nstate=int(p.get("nstate", 10)), pt2=int(p.get("pt2", 0)),
                 eps2=float(p.get("eps2", 0.0)))
     return (s, freq, cap, order, modes, vals)
+
+
+def serve(requests, slots: int = 8, reserve_bytes: float = 8e9, device: int = 0,
+          max_states: int = 256, max_basis: int = 0, max_pert: int = 0):
+    """Run many independent solves on one GPU with continuous batching (vhci_serve).
+    `requests` is a list of (input_path, arrival_seconds).  Returns (summary dict, list of
+    per-request dicts: status, energies, basis size, |P|, arrival/admit/done times, message)."""
+    n = len(requests)
+    reqs = (Request * n)()
+    keep = []
+    for i, (path, t) in enumerate(requests):
+        b = str(path).encode()
+        keep.append(b)
+        reqs[i].input_path = b
+        reqs[i].problem = None
+        reqs[i].arrival_s = float(t)
+    so = ServeOpts()
+    lib().vhci_default_serve_opts(ctypes.byref(so))
+    so.device, so.slots, so.reserve_bytes, so.max_states = device, slots, reserve_bytes, max_states
+    so.max_basis, so.max_pert = max_basis, max_pert
+    res = (Result * n)()
+    E = np.zeros(n * max_states)
+    summ = ServeSummary()
+    st = lib().vhci_serve(reqs, n, ctypes.byref(so), res, _ptr(E, ctypes.c_double),
+                          ctypes.byref(summ))
+    if st not in (OK, E_STATE):
+        raise VhciError(st, "vhci_serve")
+    out = []
+    for i in range(n):
+        r = res[i]
+        out.append({"status": r.status, "worker": r.worker, "retries": r.retries,
+                    "E": E[i * max_states: i * max_states + r.n_energies].copy(),
+                    "n_basis": r.n_basis, "n_pert": r.n_pert, "t_admit": r.t_admit,
+                    "t_done": r.t_done, "arrival": float(requests[i][1]),
+                    "message": r.message.decode(errors="replace")})
+    return ({"status": st, "wall_s": summ.wall_s, "completed": summ.completed,
+             "failed": summ.failed, "peak_in_flight": summ.peak_in_flight}, out)
 
 
 def solve(path: str, precision: int = 0, **opts) -> dict:

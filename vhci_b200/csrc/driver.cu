@@ -26,6 +26,9 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
   // perturber space: heat-bath screened states outside the basis (PT2.cpp:29-50)
   VTRY(generate_new_set(c, eps2));
   const int64_t np = c->nsel;
+  if (c->o.max_pert > 0 && np > c->o.max_pert)
+    return fail(c, VHCI_E_LIMIT, "perturber space of " + std::to_string(np) +
+                                     " states exceeds max_pert " + std::to_string(c->o.max_pert));
   const KeyLayout L = c->L;
   std::vector<double> dE(nopt, 0.0);
   c->stats.pt2_perturbers += np;
@@ -199,6 +202,10 @@ vhci_status vhci_hci(vhci_ctx* c, const char* checkpoint_path, vhci_iter_cb cb, 
       if (v) std::cout << " Performing HCI iteration: " << iter << std::endl;
       int64_t nnew = 0;
       VTRY(vhci_select(c, c->M.eps1, 0, &nnew));
+      if (c->o.max_basis > 0 && (double)nnew / (double)c->n > 0.01 && c->n + nnew > c->o.max_basis)
+        return fail(c, VHCI_E_LIMIT, "basis of " + std::to_string(c->n + nnew) +
+                                         " states would exceed max_basis " +
+                                         std::to_string(c->o.max_basis));
       if ((double)nnew / (double)c->n <= 0.01) {
         if (v) std::cout << " Basis converged after " << iter - 1 << " iterations and contains "
                          << c->n << " product states." << std::endl;

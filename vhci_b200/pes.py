@@ -211,11 +211,15 @@ def write_config(path: str, config: int, run: RunSettings | None = None) -> None
 
 def serving_request(request: int):
     """One request of the mixed serving stream: Nm in {6..24}, Nstate in {10..100}, eps1 log-uniform
-    in [0.3, 3], PT2 on with eps2 = 0.1 * eps1.  Returns (PES, RunSettings)."""
+    in [0.3, 3], PT2 on with eps2 = 0.1 * eps1.  The settings come from the request's own stream;
+    the PES is redrawn (seed + 100000 j) until it passes `admissible`.  Returns (PES, RunSettings)."""
     rng = np.random.Generator(np.random.PCG64(config_seed(3, request) + 500))
     nm = int(rng.integers(6, 25))
     nstate = int(rng.integers(10, 101))
     eps1 = float("%.6f" % math.exp(rng.uniform(math.log(0.3), math.log(3.0))))
     eps2 = float("%.6f" % (0.1 * eps1))
-    pes = generate(PESSpec(nm), config_seed(3, request))
-    return pes, RunSettings(eps1=eps1, nstate=nstate, pt2=1, eps2=eps2)
+    for j in range(200):
+        pes = generate(PESSpec(nm), config_seed(3, request) + 100000 * j)
+        if admissible(pes):
+            return pes, RunSettings(eps1=eps1, nstate=nstate, pt2=1, eps2=eps2)
+    raise RuntimeError(f"no admissible PES for serving request {request}")
