@@ -37,6 +37,10 @@ ConnDev conn_view(vhci_ctx* c) {
   d.T = c->T.p;
   d.freq = c->freq.p;
   d.nm = c->M.nm;
+  d.lkey = c->lkey.p;
+  d.lseg = c->lseg.p;
+  d.lmask = c->lmask;
+  d.maxl = c->maxl;
   return d;
 }
 
@@ -127,6 +131,27 @@ int upload_tables(vhci_ctx* c) {
   }
   VTRY(upload(c, c->groups, g));
   VTRY(upload(c, c->wdelta, wd));
+  // lowered-mode segment index: open addressing on the segment keys, load <= 1/2
+  {
+    const ConnTables& t = c->conn;
+    const size_t nseg = t.seg_key.size();
+    size_t P = 64;
+    while (P < 2 * nseg) P <<= 1;
+    std::vector<uint64_t> lk(P, 0);
+    std::vector<int32_t> ls(2 * P, 0);
+    for (size_t q = 0; q < nseg; ++q) {
+      size_t h = mix64(t.seg_key[q]) & (P - 1);
+      while (lk[h] != 0) h = (h + 1) & (P - 1);
+      lk[h] = t.seg_key[q];
+      ls[2 * h] = t.seg_begin[q];
+      ls[2 * h + 1] = t.seg_begin[q + 1] - t.seg_begin[q];
+    }
+    VTRY(upload(c, c->lkey, lk));
+    VTRY(upload(c, c->lseg, ls));
+    c->lmask = (uint32_t)(P - 1);
+    // the index covers up to 126 modes and 6 lowered modes (the key packs 7 bits per mode)
+    c->maxl = (c->M.nm <= 126 && t.max_lowered <= 6 && nseg > 0) ? t.max_lowered : -1;
+  }
   VTRY(upload(c, c->terms, conv(c->conn.terms)));
   VTRY(upload(c, c->dterms, conv(c->conn.diag_terms)));
   VTRY(upload(c, c->T, T));

@@ -37,6 +37,10 @@ struct DBuf {
     p = nullptr;
     cap = 0;
   }
+  void swap(DBuf& o) {
+    std::swap(p, o.p);
+    std::swap(cap, o.cap);
+  }
 };
 
 struct Status {
@@ -70,6 +74,10 @@ struct vhci_ctx {
   // tables on device
   vhci::DBuf<vhci::GroupDev> groups;
   vhci::DBuf<int64_t> wdelta;
+  vhci::DBuf<uint64_t> lkey;       // lowered-mode segment index (see ConnDev)
+  vhci::DBuf<int32_t> lseg;
+  uint32_t lmask = 0;
+  int maxl = -1;
   vhci::DBuf<vhci::TermDev> terms, dterms;
   vhci::DBuf<double> T, freq;
   vhci::DBuf<vhci::HBDev> hbdev;

@@ -33,6 +33,10 @@ __global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ key
                                                 double* __restrict__ val,
                                                 float* __restrict__ valf,
                                                 double* __restrict__ diag) {
+  __shared__ uint32_t s_binom[kBinomElems];
+  __shared__ uint8_t s_exc[8][128];
+  fill_binom(s_binom);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
@@ -41,11 +45,10 @@ __global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ key
     load_key<W>(keys, i, k);
     const int64_t pos = FILL ? rowptr[i] : 0;
     int cnt = 0;
-    for (int64_t u0 = 0; u0 < cd.ngroups; u0 += 32) {
-      const int64_t u = u0 + lane;
+    for_each_group<W>(cd, k, L, s_exc[threadIdx.x >> 5], s_binom, [&](int64_t u) {
       int64_t j = -1;
       GroupDev g;
-      if (u < cd.ngroups) {
+      if (u >= 0) {
         g = cd.groups[u];
         uint64_t t[W];
         if (group_target<W>(cd, u, g, k, L, t)) j = hash_find<W>(basis, t, key_hash<W>(t));
@@ -58,7 +61,7 @@ __global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ key
         if (valf) valf[p] = (float)v; else val[p] = v;
       }
       cnt += __popc(b);
-    }
+    });
     if (lane == 0) {
       if (FILL) diag[i] = diag_value<W>(cd, k, L);
       else rowcnt[i] = cnt;

@@ -30,18 +30,22 @@ __global__ void __launch_bounds__(256) k_pt2_gen(const uint64_t* __restrict__ ke
                                                  const int64_t* __restrict__ arowptr,
                                                  int32_t* __restrict__ ecol,
                                                  double* __restrict__ eval) {
-  const int lane = threadIdx.x & 31;
+  __shared__ uint32_t s_binom[kBinomElems];
+  __shared__ uint8_t s_exc[8][128];
+  fill_binom(s_binom);
+  __syncthreads();
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
        i += warps) {
     uint64_t k[W];
     load_key<W>(keys, i, k);
-    for (int64_t u = lane; u < cd.ngroups; u += 32) {
+    for_each_group<W>(cd, k, L, s_exc[threadIdx.x >> 5], s_binom, [&](int64_t u) {
+      if (u < 0) return;
       const GroupDev g = cd.groups[u];
       uint64_t t[W];
-      if (!group_target<W>(cd, u, g, k, L, t)) continue;
+      if (!group_target<W>(cd, u, g, k, L, t)) return;
       const int64_t a = hash_find<W>(pert, t, key_hash<W>(t));
-      if (a < a_lo || a >= a_hi) continue;
+      if (a < a_lo || a >= a_hi) return;
       if (!FILL) {
         atomicAdd(acount + (a - a_lo), 1);
       } else {
@@ -49,7 +53,7 @@ __global__ void __launch_bounds__(256) k_pt2_gen(const uint64_t* __restrict__ ke
         ecol[p] = (int32_t)i;
         eval[p] = group_value<W>(cd, g.tb, g.te, k, L);
       }
-    }
+    });
   }
 }
 

@@ -322,8 +322,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       if (plevel)
         std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
                      (long long)n, k, b, cyc + 1, steps, t_spmm, t_orth, t_rr, msince(t_start));
-      VCK(c->X.reserve((size_t)n * kk, s));
-      VCK(cudaMemcpyAsync(c->X.p, w.Xb.p, (size_t)n * kk * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      c->X.swap(w.Xb);  // hand the Ritz block over; the old X buffer is released with w
       c->ldx = kk;
       c->nvec = nk;
       c->x_rows = n;
@@ -357,8 +356,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       exhausted = true;
     }
     if (exhausted) {
-      VCK(c->X.reserve((size_t)n * kk, s));
-      VCK(cudaMemcpyAsync(c->X.p, w.Xb.p, (size_t)n * kk * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      c->X.swap(w.Xb);  // hand the Ritz block over; the old X buffer is released with w
       c->ldx = kk;
       c->nvec = nk;
       c->x_rows = n;

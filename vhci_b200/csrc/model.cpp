@@ -276,11 +276,36 @@ void build_conn_tables(const Model& m, ConnTables& t) {
         per_group[gid].push_back(tm);
       });
     }
-  for (size_t g = 0; g < t.groups.size(); ++g) {
-    t.groups[g].term_begin = (int)t.terms.size();
-    t.terms.insert(t.terms.end(), per_group[g].begin(), per_group[g].end());
-    t.groups[g].term_end = (int)t.terms.size();
+  // order groups by lowered-mode key (stable: first-seen order within a segment)
+  const size_t ng = t.groups.size();
+  std::vector<uint64_t> gkey(ng);
+  t.max_lowered = 0;
+  for (size_t g = 0; g < ng; ++g) {
+    int low[kMaxOrder], r = 0;
+    for (int k = 0; k < t.groups[g].nchg; ++k)
+      if (t.groups[g].delta[k] < 0) low[r++] = t.groups[g].mode[k];  // modes are ascending
+    gkey[g] = lowered_key(r, low);
+    t.max_lowered = std::max(t.max_lowered, r);
   }
+  std::vector<size_t> ord(ng);
+  for (size_t g = 0; g < ng; ++g) ord[g] = g;
+  std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return gkey[a] < gkey[b]; });
+  std::vector<Group> sorted(ng);
+  t.seg_key.clear();
+  t.seg_begin.clear();
+  for (size_t i = 0; i < ng; ++i) {
+    const size_t g = ord[i];
+    sorted[i] = t.groups[g];
+    if (t.seg_key.empty() || t.seg_key.back() != gkey[g]) {
+      t.seg_key.push_back(gkey[g]);
+      t.seg_begin.push_back((int)i);
+    }
+    sorted[i].term_begin = (int)t.terms.size();
+    t.terms.insert(t.terms.end(), per_group[g].begin(), per_group[g].end());
+    sorted[i].term_end = (int)t.terms.size();
+  }
+  t.seg_begin.push_back((int)ng);
+  t.groups.swap(sorted);
 }
 
 void build_hb_entries(const Model& m, std::vector<HBEntry>& e, std::vector<int64_t>& cum) {

@@ -62,10 +62,25 @@ struct Group {
   int term_begin = 0, term_end = 0;
 };
 
+// Key of the set of modes a change vector lowers (delta < 0), modes ascending:
+// (r + 1) | sum_i (mode_i + 1) << (3 + 7 i), r <= 6 lowered modes, modes < 127.
+inline uint64_t lowered_key(int r, const int* modes_ascending) {
+  uint64_t key = (uint64_t)(r + 1);
+  for (int i = 0; i < r; ++i) key |= (uint64_t)(modes_ascending[i] + 1) << (3 + 7 * i);
+  return key;
+}
+
+// Groups are ordered by the key of their lowered-mode set, so the groups that lower one mode set
+// form one segment.  A state can only move by a group whose lowered modes are all excited in it;
+// enumerating the subsets of a state's excited modes and visiting their segments skips every
+// group that lowers an unexcited mode.
 struct ConnTables {
-  std::vector<Group> groups;     // off-diagonal groups
+  std::vector<Group> groups;     // off-diagonal groups, ordered by lowered-mode key
   std::vector<Term> terms;       // terms of the off-diagonal groups, contiguous per group
   std::vector<Term> diag_terms;  // Delta = 0 terms (quartic then sextic, input order)
+  std::vector<uint64_t> seg_key; // lowered-mode key of each segment (ascending)
+  std::vector<int> seg_begin;    // first group of each segment, plus the end
+  int max_lowered = 0;           // most modes one group lowers
 };
 void build_conn_tables(const Model& m, ConnTables& t);
 

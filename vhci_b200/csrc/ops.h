@@ -49,6 +49,12 @@ struct ConnDev {            // connection tables on device
   const double* T;          // ladder table, (qmax+1) stride
   const double* freq;       // [nm]
   int nm;
+  // lowered-mode index: open-addressing table of the group segments (groups are ordered by the
+  // key of the modes they lower; see ConnTables)
+  const uint64_t* lkey;     // [lmask + 1] segment keys, 0 = empty slot
+  const int32_t* lseg;      // [2 (lmask + 1)] first group and group count of the segment
+  uint32_t lmask;
+  int maxl;                 // most modes one group lowers; -1: no index, visit every group
 };
 
 struct HBTable {
