@@ -196,3 +196,27 @@ def test_key_layout_8bit_for_high_quanta(api):
     with api.VHCI(g["input"]) as v:
         assert v.info.key_bits == 8
         assert int(v.basis().max()) == 25
+
+
+# ---- column-panelled product (the path large bases take) ------------------------------------
+
+def test_panelled_product_matches_csr(monkeypatch):
+    """Forcing small column panels: the product and a whole solve agree with the single-pass
+    product (same entries, summed per panel)."""
+    from vhci_b200 import api
+    g = load_golden("syn_m8_sextic_pt2")
+    monkeypatch.setenv("VHCI_PANELS", "0")
+    ref = api.solve(g["input"])
+    with api.VHCI(g["input"]) as v:
+        v.hci()
+        X = np.random.default_rng(3).standard_normal((v.n, 24))
+        Y0 = v.apply_h(X)
+    monkeypatch.delenv("VHCI_PANELS")
+    monkeypatch.setenv("VHCI_PANEL_MB", "0.03")     # about 230 rows per panel
+    got = api.solve(g["input"])
+    with api.VHCI(g["input"]) as v:
+        v.hci()
+        Y1 = v.apply_h(X)
+    assert np.allclose(Y1, Y0, rtol=1e-13, atol=1e-9)
+    assert got["n_basis"] == ref["n_basis"] and got["n_pert"] == ref["n_pert"]
+    assert np.abs(got["E"] - ref["E"]).max() < 1e-8

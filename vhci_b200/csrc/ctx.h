@@ -93,6 +93,13 @@ struct vhci_ctx {
   vhci::DBuf<double> val;
   vhci::DBuf<float> valf;
   vhci::DBuf<double> diag;
+  // column panels of the off-diagonal entries (built with H when the gathered block outgrows L2)
+  int npanel = 0;
+  int64_t panel_cw = 0;
+  vhci::DBuf<int64_t> prow;
+  vhci::DBuf<int32_t> pcol;
+  vhci::DBuf<double> pval;
+  vhci::DBuf<float> pvalf;
 
   // eigenpairs: X is row-major x_rows x ldx, nvec columns valid
   int nvec = 0, ldx = 0;

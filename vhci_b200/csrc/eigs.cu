@@ -141,8 +141,7 @@ int apply_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
   VCK(cudaEventCreate(&e0));
   VCK(cudaEventCreate(&e1));
   VCK(cudaEventRecord(e0, c->st));
-  spmm(c->n, c->rowptr.p, c->col.p, c->o.precision == 1 ? nullptr : c->val.p,
-       c->o.precision == 1 ? c->valf.p : nullptr, c->diag.p, X, ldx, b, Y, ldy, c->st);
+  spmm_h(c, X, ldx, b, Y, ldy);
   VCK(cudaEventRecord(e1, c->st));
   VCK(cudaEventSynchronize(e1));
   VCK(cudaGetLastError());

@@ -43,6 +43,10 @@ int append_keys(vhci_ctx* c, const uint64_t* dkeys, int64_t m);
 int generate_new_set(vhci_ctx* c, double eps);
 
 int build_h(vhci_ctx* c);
+// Y = H X on the context's stream, through the column panels when they are built.
+void spmm_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy);
+// Device memory a new allocation can use: free memory plus the pool's idle reserve.
+double device_available(vhci_ctx* c);
 // Lowest k eigenpairs; dense_all keeps every eigenpair of a dense solve (first HCI step).
 int eigs(vhci_ctx* c, int k);
 int dense_eigs(vhci_ctx* c, int keep);

@@ -173,13 +173,13 @@ __global__ void __launch_bounds__(256) k_spmm_panel(int64_t n, const int64_t* __
 // lanes that own one column each and walk the row's entries together (the entry loads are
 // broadcasts within the group and L1 hits across consecutive entries), so the inner loop has no
 // shuffles: two cached loads, one gathered load and one FMA per entry.
-template <int BP, typename VT, bool CG>
+template <int BP, typename VT, bool CG, int U = 4>
 __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __restrict__ rowptr,
                                                    const int32_t* __restrict__ col,
                                                    const VT* __restrict__ val,
                                                    const double* __restrict__ diag,
                                                    const double* __restrict__ X, int ldx, int bp,
-                                                   double* __restrict__ Y, int ldy) {
+                                                   double* __restrict__ Y, int ldy, int accum) {
   constexpr int G = 32 / BP;
   const int lane = threadIdx.x & 31;
   const int grp = lane / BP, cc = lane % BP;
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
        i < n; i += stride) {
     const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
     double acc = 0.0;
-    if (active) {
+    if (active && (!accum || end > beg)) {
       auto gx = [&](int j) {
         const double* xp = X + (int64_t)j * ldx + cc;
         return CG ? __ldcg(xp) : __ldg(xp);
@@ -199,6 +199,26 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
         // entries four at a time: one 16-byte column load and two 16-byte value loads, each a
         // broadcast within the group, after a scalar prologue to 4-entry alignment
         for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
+        if constexpr (U == 8) {  // eight gathers in flight per lane
+          for (; e + 8 <= end; e += 8) {
+            const int4 ja = __ldg(reinterpret_cast<const int4*>(col + e));
+            const int4 jb = __ldg(reinterpret_cast<const int4*>(col + e + 4));
+            const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + e));
+            const double2 v23 = __ldg(reinterpret_cast<const double2*>(val + e + 2));
+            const double2 v45 = __ldg(reinterpret_cast<const double2*>(val + e + 4));
+            const double2 v67 = __ldg(reinterpret_cast<const double2*>(val + e + 6));
+            const double x0 = gx(ja.x), x1 = gx(ja.y), x2 = gx(ja.z), x3 = gx(ja.w);
+            const double x4 = gx(jb.x), x5 = gx(jb.y), x6 = gx(jb.z), x7 = gx(jb.w);
+            acc = fma(v01.x, x0, acc);
+            acc = fma(v01.y, x1, acc);
+            acc = fma(v23.x, x2, acc);
+            acc = fma(v23.y, x3, acc);
+            acc = fma(v45.x, x4, acc);
+            acc = fma(v45.y, x5, acc);
+            acc = fma(v67.x, x6, acc);
+            acc = fma(v67.y, x7, acc);
+          }
+        }
         for (; e + 4 <= end; e += 4) {
           const int4 j4 = __ldg(reinterpret_cast<const int4*>(col + e));
           const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + e));
@@ -212,6 +232,24 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
       } else {
         // FP32 values: one 16-byte column load and one 16-byte value load per four entries
         for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
+        if constexpr (U == 8) {
+          for (; e + 8 <= end; e += 8) {
+            const int4 ja = __ldg(reinterpret_cast<const int4*>(col + e));
+            const int4 jb = __ldg(reinterpret_cast<const int4*>(col + e + 4));
+            const float4 va = __ldg(reinterpret_cast<const float4*>(val + e));
+            const float4 vb = __ldg(reinterpret_cast<const float4*>(val + e + 4));
+            const double x0 = gx(ja.x), x1 = gx(ja.y), x2 = gx(ja.z), x3 = gx(ja.w);
+            const double x4 = gx(jb.x), x5 = gx(jb.y), x6 = gx(jb.z), x7 = gx(jb.w);
+            acc = fma((double)va.x, x0, acc);
+            acc = fma((double)va.y, x1, acc);
+            acc = fma((double)va.z, x2, acc);
+            acc = fma((double)va.w, x3, acc);
+            acc = fma((double)vb.x, x4, acc);
+            acc = fma((double)vb.y, x5, acc);
+            acc = fma((double)vb.z, x6, acc);
+            acc = fma((double)vb.w, x7, acc);
+          }
+        }
         for (; e + 4 <= end; e += 4) {
           const int4 j4 = __ldg(reinterpret_cast<const int4*>(col + e));
           const float4 v4 = __ldg(reinterpret_cast<const float4*>(val + e));
@@ -224,7 +262,8 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
       }
 #pragma unroll 4
       for (; e < end; ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
-      Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
+      if (accum) Y[i * ldy + cc] += acc;  // a later column panel: add this panel's entries
+      else Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
     }
   }
 }
@@ -271,6 +310,28 @@ __global__ void __launch_bounds__(256) k_spmm_rg(int64_t n, const int64_t* __res
 constexpr double kSpmmL2Budget = 64e6;
 
 template <typename VT>
+void spmm_rows_launch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
+                      const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
+                      int accum, cudaStream_t s) {
+  const int BP = b <= 8 ? 8 : (b <= 16 ? 16 : 32);
+  const int gr = grid_for(n * BP, 256, 148 * 16);
+  // eight entries per iteration (eight gathers in flight per lane) by default; measured 11-14 %
+  // faster than four on the 380k- and 6.1M-state matrices.  VHCI_SPMM_UNROLL=4 selects four.
+  const char* ue = std::getenv("VHCI_SPMM_UNROLL");
+  const bool u8 = !(ue && std::atoi(ue) == 4);
+  for (int c0 = 0; c0 < b; c0 += BP) {
+    const int bp = std::min(BP, b - c0);
+    note_launch();
+#define VHCI_ROWS(BPV, UV) k_spmm_rows<BPV, VT, false, UV><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, accum)
+    if (BP == 32) { if (u8) VHCI_ROWS(32, 8); else VHCI_ROWS(32, 4); }
+    else if (BP == 16) { if (u8) VHCI_ROWS(16, 8); else VHCI_ROWS(16, 4); }
+    else { if (u8) VHCI_ROWS(8, 8); else VHCI_ROWS(8, 4); }
+#undef VHCI_ROWS
+  }
+}
+
+
+template <typename VT>
 void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
                    const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
                    cudaStream_t s) {
@@ -303,15 +364,11 @@ void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const V
       } else if (form == "rows_cg") {
         if (BP == 4) BP = 8;
         const int gr = grid_for(n * BP, 256, 148 * 16);
-        if (BP == 32) { note_launch(); k_spmm_rows<32, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else if (BP == 16) { note_launch(); k_spmm_rows<16, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else { note_launch(); k_spmm_rows<8, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        if (BP == 32) { note_launch(); k_spmm_rows<32, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0); }
+        else if (BP == 16) { note_launch(); k_spmm_rows<16, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0); }
+        else { note_launch(); k_spmm_rows<8, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0); }
       } else {
-        if (BP == 4) BP = 8;
-        const int gr = grid_for(n * BP, 256, 148 * 16);
-        if (BP == 32) { note_launch(); k_spmm_rows<32, VT, false><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else if (BP == 16) { note_launch(); k_spmm_rows<16, VT, false><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else { note_launch(); k_spmm_rows<8, VT, false><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
+        spmm_rows_launch<VT>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0, s);
       }
     }
     return;
@@ -460,6 +517,97 @@ void hbuild_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, C
                  cudaStream_t s) {
   if (n <= 0) return;
   VHCI_DISPATCH_W(L.W, hbuild_fill_launch, keys, n, L, basis, cd, rowptr, col, val, valf, diag, s);
+}
+
+// ---- column panels: the off-diagonal entries regrouped by column range -----------------------
+// When the gathered block no longer fits in L2, the product runs once per column panel, so the
+// rows gathered in one pass (one panel of the block) stay L2-resident while H streams once.
+// Layout: entries of panel p for row i at [prow[p n + i], prow[p n + i + 1]); within a (panel,
+// row) cell entries keep their CSR order, so the product is deterministic.
+
+namespace {
+
+// cnt[p n + i] = entries of row i in column panel p (cnt zeroed by the caller).
+__global__ void __launch_bounds__(256) k_panel_count(int64_t n, const int64_t* __restrict__ rowptr,
+                                                     const int32_t* __restrict__ col, int64_t cw,
+                                                     int32_t* __restrict__ cnt) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += warps) {
+    const int64_t beg = rowptr[i], end = rowptr[i + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      const bool v = e < end;
+      const int p = v ? (int)(col[e] / cw) : -1;
+      const unsigned peers = __match_any_sync(full, p);
+      if (v && (peers & lanemask_lt()) == 0) atomicAdd(cnt + (int64_t)p * n + i, __popc(peers));
+    }
+  }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(256) k_panel_fill(int64_t n, const int64_t* __restrict__ rowptr,
+                                                    const int32_t* __restrict__ col,
+                                                    const VT* __restrict__ val, int64_t cw, int P,
+                                                    const int64_t* __restrict__ prow,
+                                                    int32_t* __restrict__ pcol,
+                                                    VT* __restrict__ pval) {
+  __shared__ int s_run[8][kMaxPanels];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int* run = s_run[threadIdx.x >> 5];
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += warps) {
+    for (int p = lane; p < P; p += 32) run[p] = 0;
+    __syncwarp();
+    const int64_t beg = rowptr[i], end = rowptr[i + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      const bool v = e < end;
+      const int p = v ? (int)(col[e] / cw) : -1;
+      const unsigned peers = __match_any_sync(full, p);
+      const unsigned below = peers & lanemask_lt();
+      if (v) {
+        const int64_t pos = prow[(int64_t)p * n + i] + run[p] + __popc(below);
+        pcol[pos] = col[e];
+        pval[pos] = val[e];
+      }
+      __syncwarp();
+      if (v && below == 0) run[p] += __popc(peers);
+      __syncwarp();
+    }
+  }
+}
+
+}  // namespace
+
+void panel_count(int64_t n, const int64_t* rowptr, const int32_t* col, int64_t cw, int32_t* cnt,
+                 cudaStream_t s) {
+  if (n <= 0) return;
+  note_launch(); k_panel_count<<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(n, rowptr, col, cw, cnt);
+}
+
+void panel_fill(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
+                const float* valf, int64_t cw, int P, const int64_t* prow, int32_t* pcol,
+                double* pval, float* pvalf, cudaStream_t s) {
+  if (n <= 0) return;
+  const int g = grid_for(n * 32, 256, 148 * 8);
+  note_launch();
+  if (valf) k_panel_fill<float><<<g, 256, 0, s>>>(n, rowptr, col, valf, cw, P, prow, pcol, pvalf);
+  else k_panel_fill<double><<<g, 256, 0, s>>>(n, rowptr, col, val, cw, P, prow, pcol, pval);
+}
+
+void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, const double* pval,
+                 const float* pvalf, const double* diag, const double* X, int ldx, int b,
+                 double* Y, int ldy, cudaStream_t s) {
+  if (n <= 0 || b <= 0) return;
+  for (int p = 0; p < P; ++p) {
+    if (pvalf) spmm_rows_launch<float>(n, prow + (int64_t)p * n, pcol, pvalf, diag, X, ldx, b, Y, ldy, p > 0, s);
+    else spmm_rows_launch<double>(n, prow + (int64_t)p * n, pcol, pval, diag, X, ldx, b, Y, ldy, p > 0, s);
+  }
 }
 
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,

@@ -152,8 +152,7 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
   VCK(w.Xc.reserve((size_t)c->n * b, c->st));
   VCK(cudaEventRecord(e0, c->st));
   copy_cols(X, ldx, w.Xc.p, b, c->n, b, c->st);
-  spmm(c->n, c->rowptr.p, c->col.p, c->o.precision == 1 ? nullptr : c->val.p,
-       c->o.precision == 1 ? c->valf.p : nullptr, c->diag.p, w.Xc.p, b, b, Y, ldy, c->st);
+  spmm_h(c, w.Xc.p, b, b, Y, ldy);
   VCK(cudaEventRecord(e1, c->st));
   VCK(cudaEventSynchronize(e1));
   VCK(cudaGetLastError());

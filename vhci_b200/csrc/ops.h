@@ -112,6 +112,17 @@ void hbuild_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, 
 void hbuild_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
                  const int64_t* rowptr, int32_t* col, double* val, float* valf, double* diag,
                  cudaStream_t s);
+// Column panels of the off-diagonal CSR (at most kMaxPanels): entries of panel p (columns
+// [p cw, (p+1) cw)) for row i at [prow[p n + i], prow[p n + i + 1]).
+constexpr int kMaxPanels = 64;
+void panel_count(int64_t n, const int64_t* rowptr, const int32_t* col, int64_t cw, int32_t* cnt,
+                 cudaStream_t s);
+void panel_fill(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
+                const float* valf, int64_t cw, int P, const int64_t* prow, int32_t* pcol,
+                double* pval, float* pvalf, cudaStream_t s);
+void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, const double* pval,
+                 const float* pvalf, const double* diag, const double* X, int ldx, int b,
+                 double* Y, int ldy, cudaStream_t s);
 // Y[:, 0:b] = H X[:, 0:b] with H = diag + off-diagonal CSR (FP64 or FP32 values).
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
           const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
