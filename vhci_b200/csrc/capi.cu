@@ -318,10 +318,9 @@ void spmm_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
          c->diag.p, X, ldx, b, Y, ldy, c->st);
 }
 
-// Column panels for the product: one 16-column FP64 block row is 128 bytes.  Panels are built when
-// the block's rows exceed 80 MB (past that they no longer stay in the 126 MB L2 beside the matrix
-// stream); each panel's rows take about 96 MB (VHCI_PANEL_MB sets the panel size and forces
-// panels at any size; VHCI_PANELS=0 turns them off).  On the 6.1M-state, 1.17e9-entry matrix
+// Column panels for the product: one 16-column FP64 block row is 128 bytes, and each panel's rows
+// take about 96 MB of the 126 MB L2, so panels start at two when the block's rows exceed 96 MB
+// (N > 750k).  VHCI_PANEL_MB sets the panel size; VHCI_PANELS=0 turns panels off.  On the 6.1M-state, 1.17e9-entry matrix
 // 96 MB panels measured 3 % faster than one pass and 48 MB ones no faster: the product there is
 // bound by the dependent index-then-gather loads more than by where the block rows live.  Skipped when the regrouped copy does not fit
 // in free device memory.
@@ -331,11 +330,7 @@ static int build_panels(vhci_ctx* c) {
   if (const char* e = std::getenv("VHCI_PANELS"))
     if (std::atoi(e) == 0) return VHCI_OK;
   double pbytes = 96e6;
-  if (const char* e = std::getenv("VHCI_PANEL_MB")) {
-    pbytes = std::max(0.01, std::atof(e)) * 1e6;
-  } else if ((double)n * 128.0 <= 80e6) {
-    return VHCI_OK;  // the whole block stays L2-resident: one pass
-  }
+  if (const char* e = std::getenv("VHCI_PANEL_MB")) pbytes = std::max(0.01, std::atof(e)) * 1e6;
   int P = (int)std::ceil((double)n * 128.0 / pbytes);
   if (P < 2 || c->nnz == 0) return VHCI_OK;
   P = std::min(P, kMaxPanels);
