@@ -220,3 +220,19 @@ def test_panelled_product_matches_csr(monkeypatch):
     assert np.allclose(Y1, Y0, rtol=1e-13, atol=1e-9)
     assert got["n_basis"] == ref["n_basis"] and got["n_pert"] == ref["n_pert"]
     assert np.abs(got["E"] - ref["E"]).max() < 1e-8
+
+
+def test_lean_lanczos_end_to_end_workload0(monkeypatch):
+    """The memory-lean eigensolver (only Q stored, residuals from the Krylov relation, confirmed
+    explicitly) on workload 0 (35,229 states, Nstate 50): the reference program's levels and
+    basis size, and the default eigensolver's energies."""
+    from vhci_b200 import api
+    g = load_golden("workload0")
+    ref = api.solve(g["input"])
+    monkeypatch.setenv("VHCI_LANCZOS_LEAN", "1")
+    got = api.solve(g["input"])
+    assert got["n_basis"] == g["log"]["final_basis"] == ref["n_basis"]
+    assert np.abs(got["E"] - ref["E"]).max() < 1e-6
+    lev = levels_of(got["E"])
+    levels = np.array(g["levels"])
+    assert np.abs(lev[:len(levels)] - levels).max() <= E_TOL

@@ -340,7 +340,9 @@ static int build_panels(vhci_ctx* c) {
   const double sval = c->o.precision == 1 ? 4.0 : 8.0;
   const double need = (double)c->nnz * (4.0 + sval) + (pn + 1) * 8.0 + pn * 4.0 +
                       scan_tmp_elems(pn) * 8.0 + 2e9;
-  if (need > device_available(c)) return VHCI_OK;  // no room: the plain product serves
+  // the eigensolver's smallest working set must still fit after the panels: the panels are an
+  // optimisation, the Lanczos basis is not
+  if (need + lanczos_min_bytes(c, c->M.nstate) > device_available(c)) return VHCI_OK;
   DBuf<int32_t> cnt;
   DBuf<int64_t> tmp;
   VCK(cnt.reserve(pn, c->st));
@@ -379,6 +381,24 @@ int build_h(vhci_ctx* c) {
   int64_t nnz = 0;
   VCK(d2h(c, &nnz, c->rowptr.p + n, sizeof(int64_t)));
   VCK(cudaStreamSynchronize(c->st));
+  // the previous matrix's arrays are replaced, not grown in place: release them first so the old
+  // and new matrix never coexist
+  if ((int64_t)c->col.cap < nnz) c->col.release(c->st);
+  if ((int64_t)c->val.cap < nnz) c->val.release(c->st);
+  if ((int64_t)c->valf.cap < nnz) c->valf.release(c->st);
+  {  // admission: the matrix and the eigensolver's smallest working set must fit together
+    const double hbytes = (double)nnz * (4.0 + (c->o.precision == 1 ? 4.0 : 8.0)) + 8.0 * n;
+    const double avail = device_available(c) + 8.0 * (double)c->x_rows * c->ldx;
+    const double eig = lanczos_min_bytes(c, c->M.nstate);
+    if (hbytes + eig > avail) {
+      char msg[320];
+      std::snprintf(msg, sizeof msg,
+                    "Hamiltonian of %lld states and %lld off-diagonal entries needs %.1f GB (plus "
+                    "%.1f GB for the eigensolver); %.1f GB of device memory is available",
+                    (long long)n, (long long)nnz, hbytes / 1e9, eig / 1e9, avail / 1e9);
+      return fail(c, VHCI_E_OOM, msg);
+    }
+  }
   VCK(c->col.reserve(std::max<int64_t>(nnz, 1), c->st));
   if (c->o.precision == 1) {
     VCK(c->valf.reserve(std::max<int64_t>(nnz, 1), c->st));

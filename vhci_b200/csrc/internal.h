@@ -47,6 +47,9 @@ int build_h(vhci_ctx* c);
 void spmm_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy);
 // Device memory a new allocation can use: free memory plus the pool's idle reserve.
 double device_available(vhci_ctx* c);
+// Device bytes the block Lanczos needs for k eigenpairs on the current basis with its smallest
+// subspace (span 2).
+double lanczos_min_bytes(vhci_ctx* c, int k);
 // Lowest k eigenpairs; dense_all keeps every eigenpair of a dense solve (first HCI step).
 int eigs(vhci_ctx* c, int k);
 int dense_eigs(vhci_ctx* c, int keep);

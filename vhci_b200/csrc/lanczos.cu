@@ -181,15 +181,48 @@ int lanczos_block(int64_t n) {
   return 16;
 }
 
+// Working set of the block Lanczos for subspace factor `span`: Q and H Q (n x ld), the Ritz block
+// and its product (n x kk), the expansion block and its compact copy (n x b), in doubles.
+static double lanczos_bytes(int64_t n, int k, int span, int b) {
+  const int kk = (int)std::min<int64_t>(n, k + std::max(8, k / 10));
+  const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
+  const int ld = (mmax + b + 15) / 16 * 16;
+  return 8.0 * (double)n * (2.0 * ld + 2.0 * kk + 2.0 * b);
+}
+
+// Working set of the memory-lean variant: Q (n x ld, span 2), the expansion block, its product,
+// the compact copy (n x b each), the rotation chunk, and the output Ritz block (n x kk).
+static double lanczos_lean_bytes(int64_t n, int k, int b, int span = 2) {
+  const int kk = (int)std::min<int64_t>(n, k + std::max(8, k / 10));
+  const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
+  const int ld = (mmax + b + 15) / 16 * 16;
+  return 8.0 * (double)n * (ld + 3.0 * b + kk) + 2.6e8;
+}
+
+double lanczos_min_bytes(vhci_ctx* c, int k) {
+  return lanczos_lean_bytes(c->n, k, lanczos_block(c->n)) + 1e9;
+}
+
+int block_lanczos_lean(vhci_ctx* c, int k);
+
 int block_lanczos(vhci_ctx* c, int k) {
   const int64_t n = c->n;
   cudaStream_t s = c->st;
   const int guard = std::max(8, k / 10);
   const int kk = (int)std::min<int64_t>(n, k + guard);
   const int b = lanczos_block(n);
-  // subspace size: 3 kk + 2 b by default (VHCI_LANCZOS_SPAN overrides the factor 3)
+  // subspace size: 3 kk + 2 b by default (VHCI_LANCZOS_SPAN overrides the factor 3); a basis too
+  // large for that working set in the free device memory runs with factor 2
   int span = 3;
-  if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) span = std::max(2, std::min(8, std::atoi(e)));
+  const double avail = device_available(c);
+  if (const char* e = std::getenv("VHCI_LANCZOS_LEAN"))
+    if (std::atoi(e) == 1) return block_lanczos_lean(c, k);
+  if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) {
+    span = std::max(2, std::min(8, std::atoi(e)));
+  } else if (lanczos_bytes(n, k, 3, b) + 1e9 > avail) {
+    span = 2;
+    if (lanczos_bytes(n, k, 2, b) + 1e9 > avail) return block_lanczos_lean(c, k);
+  }
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
@@ -356,6 +389,217 @@ int block_lanczos(vhci_ctx* c, int k) {
     }
     if (exhausted) {
       c->X.swap(w.Xb);  // hand the Ritz block over; the old X buffer is released with w
+      c->ldx = kk;
+      c->nvec = nk;
+      c->x_rows = n;
+      c->E.assign(th.begin(), th.begin() + nk);
+      VCK(cudaStreamSynchronize(s));
+      w.release(s);
+      return VHCI_OK;
+    }
+  }
+  w.release(s);
+  return fail(c, VHCI_E_NOT_CONVERGED, "Error: Eigenvalues did not converge.");
+}
+
+
+// Memory-lean block Lanczos for bases whose Hamiltonian leaves too little device memory for the
+// stored H Q blocks and Ritz blocks: the same thick-restart method (subspace 3 kk + 2 b when it
+// fits, else 2 kk + 2 b), but
+//   * only Q is stored; each step's product H Q_new lives in one n x b buffer, from which the new
+//     column of T = Q^T H Q and the next block are formed at once;
+//   * convergence is judged from the Krylov relation H Q = Q T + W E_last^T (W: the pending block,
+//     orthogonal to Q): the residual of Ritz pair (theta_j, y_j) is W (y_j restricted to the last
+//     block), so ||r_j||^2 = y_last^T (W^T W) y_last needs only a p x p Gram matrix;
+//   * Ritz vectors are formed in place in Q, in row chunks, and a claimed convergence is confirmed
+//     with explicit residuals H x - theta x, block by block, before returning.
+int block_lanczos_lean(vhci_ctx* c, int k) {
+  const int64_t n = c->n;
+  cudaStream_t s = c->st;
+  const int guard = std::max(8, k / 10);
+  const int kk = (int)std::min<int64_t>(n, k + guard);
+  const int b = lanczos_block(n);
+  // the largest subspace factor (3, else 2) whose lean working set fits; the previous Ritz block
+  // (n_old x kk) is released after the start block is formed, so it counts as available
+  const double avail = device_available(c) + 8.0 * (double)c->x_rows * c->ldx;
+  const int span = lanczos_lean_bytes(n, k, b, 3) + 1e9 <= avail ? 3 : 2;
+  const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
+  const int ld = (mmax + b + 15) / 16 * 16;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  const double tol = c->o.eig_tol > 0 ? c->o.eig_tol : 1e-10;
+  const double eps23 = std::pow(DBL_EPSILON, 2.0 / 3.0);
+  const char* prof = std::getenv("VHCI_PROFILE");
+  const int plevel = prof ? std::atoi(prof) : 0;
+  const int64_t chunk = std::max<int64_t>(1024, (int64_t)(2.5e8 / (8.0 * kk)));
+  LWork w;  // Q, T, Yw, theta, W (pending block), HQ (n x b product), Xb (rotation chunk)
+  VCK(w.Q.reserve((size_t)n * ld, s));
+  VCK(w.HQ.reserve((size_t)n * b, s));
+  VCK(w.W.reserve((size_t)n * b, s));
+  VCK(w.Xb.reserve((size_t)std::min<int64_t>(n, chunk) * kk, s));
+  VCK(w.T.reserve((size_t)ld * ld, s));
+  VCK(w.Yw.reserve((size_t)ld * ld, s));
+  VCK(w.theta.reserve(ld, s));
+  const int nblk = residual_blocks(n);
+  VCK(w.part.reserve((size_t)nblk * b, s));
+  VCK(w.rn2.reserve(kk, s));
+  fill_zero(w.Q.p, n * (int64_t)ld, s);
+  VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
+
+  // start block, as in block_lanczos
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  auto urand = [&]() {
+    st = mix64(st + 0x632BE59BD9B4E019ull);
+    return ((st >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  };
+  auto nrand = [&]() { return std::sqrt(-2.0 * std::log(urand())) * std::cos(6.283185307179586 * urand()); };
+  int m = 0, p = 0;
+  std::vector<double> rnd;
+  if (c->nvec > 0 && c->x_rows > 0 && c->x_rows <= n) {
+    const int w0 = std::min(c->nvec, kk);
+    rnd.resize((size_t)w0 * b);
+    for (auto& x : rnd) x = nrand();
+    DBuf<double> R;
+    VCK(R.reserve(rnd.size(), s));
+    VCK(h2d(c, R.p, rnd.data(), rnd.size() * sizeof(double)));
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, b, (int)c->x_rows, w0, &one, R.p, w0, c->X.p,
+                    c->ldx, &zero, w.W.p, b));
+    if (c->x_rows < n) fill_zero(w.W.p + (size_t)c->x_rows * b, (n - c->x_rows) * (int64_t)b, s);
+    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    VCK(cudaStreamSynchronize(s));
+    R.release(s);
+  } else {
+    rnd.resize((size_t)n * b);
+    for (auto& x : rnd) x = nrand();
+    VCK(h2d(c, w.W.p, rnd.data(), rnd.size() * sizeof(double)));
+    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+  }
+  if (p == 0) return fail(c, VHCI_E_NOT_CONVERGED, "empty start block");
+  // the previous Ritz block is no longer needed: its memory goes to the Krylov basis
+  c->X.release(s);
+  c->nvec = 0;
+  c->x_rows = 0;
+
+  // Q[:, 0:nk] = Q[:, 0:m] Y[0:m, 0:nk], in row chunks through w.Xb
+  auto rotate = [&](int mm, int nk) -> int {
+    for (int64_t r0 = 0; r0 < n; r0 += chunk) {
+      const int64_t rows = std::min(chunk, n - r0);
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nk, (int)rows, mm, &one, w.Yw.p, ld,
+                      w.Q.p + (size_t)r0 * ld, ld, &zero, w.Xb.p, nk));
+      VCK(cudaMemcpy2DAsync(w.Q.p + (size_t)r0 * ld, ld * sizeof(double), w.Xb.p,
+                            nk * sizeof(double), nk * sizeof(double), rows,
+                            cudaMemcpyDeviceToDevice, s));
+    }
+    return VHCI_OK;
+  };
+
+  std::vector<double> th(ld), rn(kk), G, Yl;
+  const int maxcyc = c->o.eig_maxit > 0 ? c->o.eig_maxit : 1000;
+  auto t_start = std::chrono::steady_clock::now();
+  int steps = 0;
+  for (int cyc = 0; cyc < maxcyc; ++cyc) {
+    bool exhausted = false;
+    int plast = 0;  // width of the block whose product formed the pending W
+    while (true) {
+      VTRY(apply_h_l(c, w, w.Q.p + m, ld, p, w.HQ.p, b));
+      ++steps;
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m + p, p, (int)n, &one, w.Q.p, ld,
+                      w.HQ.p, b, &zero, w.T.p + (size_t)m * ld, ld));
+      m += p;
+      plast = p;
+      // pending block W = H Q_new - Q T[:, new], second Gram-Schmidt pass
+      VCK(cudaMemcpyAsync(w.W.p, w.HQ.p, (size_t)n * b * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.T.p + (size_t)(m - p) * ld,
+                      ld, w.Q.p, ld, &one, w.W.p, b));
+      VCK(w.S.reserve((size_t)m * p, s));
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, p, (int)n, &one, w.Q.p, ld, w.W.p, b,
+                      &zero, w.S.p, m));
+      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.S.p, m, w.Q.p, ld,
+                      &one, w.W.p, b));
+      if (m + b > mmax || m >= n) break;
+      int p2 = 0;
+      VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + m, ld, &p2));
+      if (p2 == 0) { exhausted = true; break; }
+      p = p2;
+    }
+    // Rayleigh-Ritz
+    c->stats.eig_iterations += 1;
+    VCK(cudaMemcpy2DAsync(w.Yw.p, ld * sizeof(double), w.T.p, ld * sizeof(double),
+                          m * sizeof(double), m, cudaMemcpyDeviceToDevice, s));
+    VTRY(syevd_l(c, w.Yw.p, m, ld, w.theta.p));
+    const int nk = std::min(kk, m);
+    const int keff = std::min(k, nk);
+    VCK(d2h(c, th.data(), w.theta.p, m * sizeof(double)));
+    // residual estimates from the pending block: G = W^T W (plast x plast), Y's last-block rows
+    VCK(w.S.reserve((size_t)plast * plast, s));
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, plast, plast, (int)n, &one, w.W.p, b, w.W.p,
+                    b, &zero, w.S.p, plast));
+    G.resize((size_t)plast * plast);
+    Yl.resize((size_t)plast * nk);
+    VCK(d2h(c, G.data(), w.S.p, G.size() * sizeof(double)));
+    VCK(cudaMemcpy2DAsync(Yl.data(), plast * sizeof(double), w.Yw.p + (m - plast), ld * sizeof(double),
+                          plast * sizeof(double), nk, cudaMemcpyDeviceToHost, s));
+    VCK(cudaStreamSynchronize(s));
+    int nconv = 0;
+    double rmax = 0.0;
+    for (int j = 0; j < keff; ++j) {
+      const double* y = Yl.data() + (size_t)j * plast;
+      double r2 = 0.0;
+      for (int a = 0; a < plast; ++a)
+        for (int q = 0; q < plast; ++q) r2 += y[a] * G[(size_t)q * plast + a] * y[q];
+      const double r = std::sqrt(std::max(r2, 0.0));
+      rmax = std::max(rmax, r);
+      if (r <= tol * std::max(eps23, std::fabs(th[j]))) ++nconv;
+    }
+    if (plevel >= 2)
+      std::fprintf(stderr, "  lean lanczos cycle %d m %d converged(est) %d/%d max|r| %.3e\n", cyc, m,
+                   nconv, keff, rmax);
+    const bool full = m >= n || exhausted;
+    VTRY(rotate(m, nk));
+    bool done = full;
+    if (!full && nconv == keff) {
+      // confirm with explicit residuals, b Ritz vectors at a time
+      done = true;
+      for (int j0 = 0; j0 < keff && done; j0 += b) {
+        const int bw = std::min(b, keff - j0);
+        // compact copy (w.Xc) and product both n x bw
+        VTRY(apply_h_l(c, w, w.Q.p + j0, ld, bw, w.HQ.p, bw));
+        residual_norms(w.Xc.p, w.HQ.p, n, bw, bw, w.theta.p + j0, w.part.p, nblk, w.rn2.p + j0, s);
+        VCK(d2h(c, rn.data() + j0, w.rn2.p + j0, bw * sizeof(double)));
+        VCK(cudaStreamSynchronize(s));
+        for (int j = j0; j < j0 + bw; ++j)
+          if (std::sqrt(std::max(rn[j], 0.0)) > tol * std::max(eps23, std::fabs(th[j]))) done = false;
+      }
+    }
+    if (done) {
+      if (plevel)
+        std::fprintf(stderr, "lanczos(lean) n %lld k %d b %d span %d cycles %d steps %d ms total %.1f\n",
+                     (long long)n, k, b, span, cyc + 1, steps,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+      w.HQ.release(s);
+      w.W.release(s);
+      w.Xb.release(s);
+      VCK(c->X.reserve((size_t)n * kk, s));
+      copy_cols(w.Q.p, ld, c->X.p, kk, n, nk, s);
+      c->ldx = kk;
+      c->nvec = nk;
+      c->x_rows = n;
+      c->E.assign(th.begin(), th.begin() + nk);
+      VCK(cudaStreamSynchronize(s));
+      w.release(s);
+      return VHCI_OK;
+    }
+    // thick restart: kept Ritz vectors Q[:, 0:nk] (already rotated), then the pending block
+    int p2 = 0;
+    VTRY(svqb_small(c, w, n, w.W.p, b, plast, w.Q.p + nk, ld, &p2));
+    std::vector<double> Th((size_t)ld * nk, 0.0);
+    for (int j = 0; j < nk; ++j) Th[(size_t)j * ld + j] = th[j];
+    VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
+    VCK(h2d(c, w.T.p, Th.data(), Th.size() * sizeof(double)));
+    m = nk;
+    p = p2;
+    if (p == 0) {  // invariant: the rotated block is exact
+      VCK(c->X.reserve((size_t)n * kk, s));
+      copy_cols(w.Q.p, ld, c->X.p, kk, n, nk, s);
       c->ldx = kk;
       c->nvec = nk;
       c->x_rows = n;
