@@ -65,6 +65,10 @@ class Info(ctypes.Structure):
                 ("h_nnz", ctypes.c_int64)]
 
 
+# void (*vhci_iter_cb)(void* user, int iteration, int64_t n_basis, double zpe)
+ITER_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double)
+
+
 class Request(ctypes.Structure):
     _fields_ = [("input_path", ctypes.c_char_p), ("problem", ctypes.c_void_p),
                 ("arrival_s", ctypes.c_double)]
@@ -351,8 +355,14 @@ class VHCI:
         self._check(lib().vhci_eigs(self.h, k, _ptr(E, ctypes.c_double)))
         return E
 
-    def hci(self, checkpoint: str | None = None):
-        self._check(lib().vhci_hci(self.h, checkpoint.encode() if checkpoint else None, None, None))
+    def hci(self, checkpoint: str | None = None, callback=None):
+        """The heat-bath procedure (vhci_hci).  callback(iteration, n_basis, zpe) runs after the
+        first dense step (iteration 0) and after every heat-bath iteration's eigensolve."""
+        cb = None
+        if callback is not None:
+            cb = ITER_CB(lambda user, it, n, zpe: callback(int(it), int(n), float(zpe)))
+        self._check(lib().vhci_hci(self.h, checkpoint.encode() if checkpoint else None,
+                                   ctypes.cast(cb, ctypes.c_void_p) if cb else None, None))
 
     def pt2(self, eps2: float | None = None):
         if eps2 is None:
