@@ -42,10 +42,10 @@ WORKLOAD_DESC = ("VHCI+PT2, synthetic PES Nm=15 (cubic p=0.5 +-10^U(0,2.5), quar
                  "+-10^U(-1,1.5)), HCI_Eps=0.5, Nstate=200, PT2_Eps=0.01, Max_quanta=2")
 # Basis size after each heat-bath iteration and |P| of the workload-1 solve (FP64 path).
 WORKLOAD_COUNTS = {"sizes": [38934, 215006, 336950, 372333, 380418], "n_pert": 6583465}
-# DRAM bytes per k_spmm_rows launch, averaged over the 1070 launches of one workload-1 solve, from
+# DRAM bytes per k_spmm_rows launch, averaged over the 1085 launches of one workload-1 solve, from
 # an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of
 # `vhci_b200/bin/vhci -n 1 -i <workload-1 input> -o <out>` on B200.
-NCU_SPMM_TRAFFIC_PER_LAUNCH = 2.896e9
+NCU_SPMM_TRAFFIC_PER_LAUNCH = 2.839e9
 
 
 def _dist():
