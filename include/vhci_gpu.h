@@ -53,8 +53,9 @@ typedef struct {
   int verbose;         /* 1: print the reference's progress lines to stdout                    */
   int host_threads;    /* host threads for host-side steps (reference -n)                       */
   int64_t pt2_chunk;   /* max perturber-Hamiltonian entries held at once (0 = automatic)        */
-  int structural_nnz;  /* 1: also count the reference's structural Hamiltonian entries for the
-                          "% sparse" log line (Ham.cpp:341-342); costs one extra pass           */
+  int structural_nnz;  /* 1: the verbose "% sparse" line uses the reference's structural count
+                          (vhci_structural_nnz; one extra counting pass per build), falling
+                          back to the stored entries when that count is unavailable           */
   int64_t max_basis;   /* 0 = no limit; else a heat-bath iteration whose selection would grow the
                           basis past this fails with VHCI_E_LIMIT before building H             */
   int64_t max_pert;    /* 0 = no limit; else PT2 fails with VHCI_E_LIMIT when the screened
@@ -151,8 +152,11 @@ vhci_status vhci_get_selected(const vhci_ctx* c, uint8_t* quanta, int64_t cap, i
 vhci_status vhci_build_h(vhci_ctx* c, int64_t* nnz);
 /* Copy the Hamiltonian out as CSR with columns ascending in every row (nnz from build_h). */
 vhci_status vhci_get_h_csr(const vhci_ctx* c, int64_t* rowptr, int32_t* col, double* val);
-/* Structural entry count of the reference's pair loop (every pair passing its quanta gates),
- * for the "% sparse" line (Ham.cpp:341-342). */
+/* Entry count of the reference's stored Hamiltonian pattern (Ham.cpp:236-344): the diagonal plus
+ * every ordered pair of basis states whose quanta pass its gates, structural zeros included; the
+ * "% sparse" line prints 100 (1 - count / N^2) (Ham.cpp:341-342).  Works on the current basis
+ * (no Hamiltonian needed); VHCI_E_LIMIT when the gates admit more than 2,000,000 change patterns
+ * (many modes with 6th-order terms). */
 vhci_status vhci_structural_nnz(vhci_ctx* c, int64_t* nnz);
 
 /* Y = H X for b host vectors (n x b, column-major) with the current Hamiltonian (built on first

@@ -63,7 +63,8 @@ def _parse_assign(s):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["clo2_vhci_pt2", "syn_m6_pt2", "clo2_vci"])
+@pytest.mark.parametrize("case", ["clo2_vhci_pt2", "syn_m6_pt2", "clo2_vci", "syn_m8_sextic_pt2",
+                                  "syn_m5_cubic_pt2"])
 def test_cli_run_matches_reference_output(tmp_path, case):
     g = load_golden(case)
     out = str(tmp_path / "freqs.dat")
@@ -83,6 +84,9 @@ def test_cli_run_matches_reference_output(tmp_path, case):
     # the reference's log numbers: basis size per iteration, perturber count
     sizes = [int(x) for x in re.findall(r"Basis size after iteration \d+ is: (\d+)", r.stdout)]
     assert sizes == g["log"]["sizes"]
+    # "% sparse" counts the reference's stored pattern, structural zeros included
+    sparse = [float(x) for x in re.findall(r"The Hamiltonian is ([0-9.]+)% sparse", r.stdout)]
+    assert sparse == g["log"]["sparse_percent"]
     if g["log"]["n_pert"]:
         assert f"Perturbative space contains {g['log']['n_pert']} states." in r.stdout
     assert not os.path.exists(os.path.join(str(tmp_path), "none"))

@@ -236,3 +236,17 @@ def test_lean_lanczos_end_to_end_workload0(monkeypatch):
     lev = levels_of(got["E"])
     levels = np.array(g["levels"])
     assert np.abs(lev[:len(levels)] - levels).max() <= E_TOL
+
+
+@pytest.mark.parametrize("case", ["syn_m8_sextic_pt2", "syn_m5_cubic_pt2", "clo2_vhci"])
+def test_structural_count_matches_oracle_pair_loop(api, case):
+    """vhci_structural_nnz on a heat-bath basis against the oracle's literal pair loop over the
+    same basis (every pair passing the reference's quanta gates, plus the diagonal)."""
+    g = load_golden(case)
+    o = O.Oracle(g["input"])
+    w, C = _oracle_first_step(o)
+    o.append_basis(o.select(C, min(o.neig, o.n), o.eps1))
+    with api.VHCI(g["input"]) as v:
+        v.set_basis(o.basis())
+        got = v.structural_nnz()
+    assert got == int(O.lib().orc_build_h_pairs(o.h))

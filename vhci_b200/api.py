@@ -316,6 +316,12 @@ class VHCI:
         self._check(lib().vhci_build_h(self.h, ctypes.byref(nnz)))
         return nnz.value
 
+    def structural_nnz(self) -> int:
+        """Entries of the reference's stored pattern on the current basis (vhci_structural_nnz)."""
+        x = ctypes.c_int64()
+        self._check(lib().vhci_structural_nnz(self.h, ctypes.byref(x)))
+        return x.value
+
     def h_csr(self):
         import scipy.sparse as sp
         n = self.n

@@ -81,8 +81,52 @@ static int upload(vhci_ctx* c, DBuf<T>& b, const std::vector<T>& h) {
 }
 
 // Layout-dependent tables (packed key deltas, ladder factors) and the layout-free ones.
+// Device form of a group set under the current key layout: group records, packed key deltas per
+// word, and the lowered-mode segment table (open addressing on the segment keys, load <= 1/2).
+static int upload_groups(vhci_ctx* c, const ConnTables& t, DevGroups& dg) {
+  const KeyLayout& L = c->L;
+  std::vector<GroupDev> g(t.groups.size());
+  std::vector<int64_t> wd(t.groups.size() * L.W, 0);
+  for (size_t u = 0; u < g.size(); ++u) {
+    const Group& s = t.groups[u];
+    GroupDev d{};
+    d.tb = s.term_begin;
+    d.te = s.term_end;
+    d.nchg = (uint8_t)s.nchg;
+    for (int k = 0; k < s.nchg; ++k) {
+      d.mode[k] = (uint8_t)s.mode[k];
+      d.delta[k] = (int8_t)s.delta[k];
+      const int w = s.mode[k] / L.mpw;
+      wd[u * L.W + w] += (int64_t)((uint64_t)(int64_t)s.delta[k] << ((s.mode[k] % L.mpw) * L.bits));
+    }
+    g[u] = d;
+  }
+  VTRY(upload(c, dg.groups, g));
+  VTRY(upload(c, dg.wdelta, wd));
+  const size_t nseg = t.seg_key.size();
+  size_t P = 64;
+  while (P < 2 * nseg) P <<= 1;
+  std::vector<uint64_t> lk(P, 0);
+  std::vector<int32_t> ls(2 * P, 0);
+  for (size_t q = 0; q < nseg; ++q) {
+    size_t h = mix64(t.seg_key[q]) & (P - 1);
+    while (lk[h] != 0) h = (h + 1) & (P - 1);
+    lk[h] = t.seg_key[q];
+    ls[2 * h] = t.seg_begin[q];
+    ls[2 * h + 1] = t.seg_begin[q + 1] - t.seg_begin[q];
+  }
+  VTRY(upload(c, dg.lkey, lk));
+  VTRY(upload(c, dg.lseg, ls));
+  dg.lmask = (uint32_t)(P - 1);
+  dg.ngroups = (int64_t)t.groups.size();
+  // the index covers up to 126 modes and 6 lowered modes (the key packs 7 bits per mode)
+  dg.maxl = (c->M.nm <= 126 && t.max_lowered <= 6 && nseg > 0) ? t.max_lowered : -1;
+  return VHCI_OK;
+}
+
 int upload_tables(vhci_ctx* c) {
   const KeyLayout& L = c->L;
+  if (c->gate_built) VTRY(upload_groups(c, c->gate, c->gate_dev));  // re-packed for the layout
   std::vector<GroupDev> g(c->conn.groups.size());
   std::vector<int64_t> wd(c->conn.groups.size() * L.W, 0);
   for (size_t u = 0; u < g.size(); ++u) {
@@ -362,6 +406,51 @@ static int build_panels(vhci_ctx* c) {
   VCK(cudaGetLastError());
   c->npanel = P;
   c->panel_cw = cw;
+  return VHCI_OK;
+}
+
+// Entries of the reference's stored Hamiltonian pattern (Ham.cpp:236-344): the diagonal plus every
+// ordered pair of basis states whose quanta differ by an admitted change (|delta|_1 = s, s even
+// <= fcmax, s odd <= fcmax - 1), connected by a force constant or not (structural zeros).  The
+// gate patterns are built once and walked with the Hamiltonian build's count pass.
+constexpr int64_t kMaxGatePatterns = 2000000;
+
+bool structural_available(vhci_ctx* c) {
+  if (!c->gate_built && !c->gate_over) {
+    if (build_gate_patterns(c->M, c->gate, kMaxGatePatterns)) {
+      if (upload_groups(c, c->gate, c->gate_dev) != VHCI_OK) return false;
+      c->gate_built = true;
+    } else {
+      c->gate_over = true;
+    }
+  }
+  return c->gate_built;
+}
+
+int structural_count(vhci_ctx* c, int64_t* out) {
+  const int64_t n = c->n;
+  if (!structural_available(c))
+    return fail(c, VHCI_E_LIMIT, "the pair gates admit more than " +
+                                     std::to_string(kMaxGatePatterns) + " change patterns");
+  ConnDev d = conn_view(c);
+  d.groups = c->gate_dev.groups.p;
+  d.wdelta = c->gate_dev.wdelta.p;
+  d.ngroups = c->gate_dev.ngroups;
+  d.lkey = c->gate_dev.lkey.p;
+  d.lseg = c->gate_dev.lseg.p;
+  d.lmask = c->gate_dev.lmask;
+  d.maxl = c->gate_dev.maxl;
+  DBuf<int64_t> sum;
+  VCK(c->rowcnt.reserve(n, c->st));
+  VCK(sum.reserve(n + 1, c->st));
+  VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(n), 1), c->st));
+  hbuild_count(c->keys.p, n, c->L, basis_view(c), d, c->rowcnt.p, c->st);
+  exclusive_scan_i32(c->rowcnt.p, sum.p, n, c->scan_tmp.p, c->st);
+  int64_t pairs = 0;
+  VCK(d2h(c, &pairs, sum.p + n, sizeof(int64_t)));
+  VCK(cudaStreamSynchronize(c->st));
+  sum.release(c->st);
+  *out = n + pairs;
   return VHCI_OK;
 }
 
@@ -774,7 +863,7 @@ vhci_status vhci_get_h_csr(const vhci_ctx* c0, int64_t* rowptr, int32_t* col, do
 
 vhci_status vhci_structural_nnz(vhci_ctx* c, int64_t* nnz) {
   if (!c || !nnz) return VHCI_E_INPUT;
-  return fail(c, VHCI_E_STATE, "structural count not available in this build");
+  return structural_count(c, nnz);
 }
 
 }  // extern "C"

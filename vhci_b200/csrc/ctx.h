@@ -43,6 +43,20 @@ struct DBuf {
   }
 };
 
+// A group set on the device (see upload_groups): records, packed key deltas, segment table.
+struct DevGroups {
+  DBuf<GroupDev> groups;
+  DBuf<int64_t> wdelta;
+  DBuf<uint64_t> lkey;
+  DBuf<int32_t> lseg;
+  uint32_t lmask = 0;
+  int maxl = -1;
+  int64_t ngroups = 0;
+  void release(cudaStream_t s) {
+    groups.release(s); wdelta.release(s); lkey.release(s); lseg.release(s);
+  }
+};
+
 struct Status {
   int code = VHCI_OK;
   std::string msg;
@@ -74,6 +88,10 @@ struct vhci_ctx {
   // tables on device
   vhci::DBuf<vhci::GroupDev> groups;
   vhci::DBuf<int64_t> wdelta;
+  // the reference's pair-gate patterns, for the structural entry count (built on first use)
+  bool gate_built = false, gate_over = false;
+  vhci::ConnTables gate;
+  vhci::DevGroups gate_dev;
   vhci::DBuf<uint64_t> lkey;       // lowered-mode segment index (see ConnDev)
   vhci::DBuf<int32_t> lseg;
   uint32_t lmask = 0;

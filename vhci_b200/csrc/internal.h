@@ -43,6 +43,9 @@ int append_keys(vhci_ctx* c, const uint64_t* dkeys, int64_t m);
 int generate_new_set(vhci_ctx* c, double eps);
 
 int build_h(vhci_ctx* c);
+// Entries of the reference's stored pattern (diagonal + gated pairs, structural zeros included).
+bool structural_available(vhci_ctx* c);
+int structural_count(vhci_ctx* c, int64_t* out);
 // Y = H X on the context's stream, through the column panels when they are built.
 void spmm_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy);
 // Device memory a new allocation can use: free memory plus the pool's idle reserve.

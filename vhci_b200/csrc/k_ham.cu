@@ -318,14 +318,16 @@ void spmm_rows_launch(int64_t n, const int64_t* rowptr, const int32_t* col, cons
   // eight entries per iteration (eight gathers in flight per lane) by default; measured 11-14 %
   // faster than four on the 380k- and 6.1M-state matrices.  VHCI_SPMM_UNROLL=4 selects four.
   const char* ue = std::getenv("VHCI_SPMM_UNROLL");
-  const bool u8 = !(ue && std::atoi(ue) == 4);
+  const int u = ue ? std::atoi(ue) : 8;
   for (int c0 = 0; c0 < b; c0 += BP) {
     const int bp = std::min(BP, b - c0);
     note_launch();
 #define VHCI_ROWS(BPV, UV) k_spmm_rows<BPV, VT, false, UV><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, accum)
-    if (BP == 32) { if (u8) VHCI_ROWS(32, 8); else VHCI_ROWS(32, 4); }
-    else if (BP == 16) { if (u8) VHCI_ROWS(16, 8); else VHCI_ROWS(16, 4); }
-    else { if (u8) VHCI_ROWS(8, 8); else VHCI_ROWS(8, 4); }
+#define VHCI_ROWS_U(BPV) do { if (u == 4) VHCI_ROWS(BPV, 4); else VHCI_ROWS(BPV, 8); } while (0)
+    if (BP == 32) VHCI_ROWS_U(32);
+    else if (BP == 16) VHCI_ROWS_U(16);
+    else VHCI_ROWS_U(8);
+#undef VHCI_ROWS_U
 #undef VHCI_ROWS
   }
 }

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <fstream>
+#include <functional>
 #include <map>
 
 namespace vhci {
@@ -230,6 +231,41 @@ bool finalize_model(Model& m, bool restart, std::string& err) {
   return true;
 }
 
+// Orders t.groups by lowered-mode key (stable: first-seen order within a segment), records the
+// segments, and lays out the terms contiguously per group (per_group: terms of each group in the
+// original order, or null for groups without terms).
+static void index_groups(ConnTables& t, const std::vector<std::vector<Term>>* per_group) {
+  const size_t ng = t.groups.size();
+  std::vector<uint64_t> gkey(ng);
+  t.max_lowered = 0;
+  for (size_t g = 0; g < ng; ++g) {
+    int low[kMaxOrder], r = 0;
+    for (int k = 0; k < t.groups[g].nchg; ++k)
+      if (t.groups[g].delta[k] < 0) low[r++] = t.groups[g].mode[k];  // modes are ascending
+    gkey[g] = lowered_key(r, low);
+    t.max_lowered = std::max(t.max_lowered, r);
+  }
+  std::vector<size_t> ord(ng);
+  for (size_t g = 0; g < ng; ++g) ord[g] = g;
+  std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return gkey[a] < gkey[b]; });
+  std::vector<Group> sorted(ng);
+  t.seg_key.clear();
+  t.seg_begin.clear();
+  for (size_t i = 0; i < ng; ++i) {
+    const size_t g = ord[i];
+    sorted[i] = t.groups[g];
+    if (t.seg_key.empty() || t.seg_key.back() != gkey[g]) {
+      t.seg_key.push_back(gkey[g]);
+      t.seg_begin.push_back((int)i);
+    }
+    sorted[i].term_begin = (int)t.terms.size();
+    if (per_group) t.terms.insert(t.terms.end(), (*per_group)[g].begin(), (*per_group)[g].end());
+    sorted[i].term_end = (int)t.terms.size();
+  }
+  t.seg_begin.push_back((int)ng);
+  t.groups.swap(sorted);
+}
+
 void build_conn_tables(const Model& m, ConnTables& t) {
   t.groups.clear(); t.terms.clear(); t.diag_terms.clear();
   std::map<std::vector<int>, int> index;         // change vector -> group id
@@ -276,36 +312,46 @@ void build_conn_tables(const Model& m, ConnTables& t) {
         per_group[gid].push_back(tm);
       });
     }
-  // order groups by lowered-mode key (stable: first-seen order within a segment)
-  const size_t ng = t.groups.size();
-  std::vector<uint64_t> gkey(ng);
-  t.max_lowered = 0;
-  for (size_t g = 0; g < ng; ++g) {
-    int low[kMaxOrder], r = 0;
-    for (int k = 0; k < t.groups[g].nchg; ++k)
-      if (t.groups[g].delta[k] < 0) low[r++] = t.groups[g].mode[k];  // modes are ascending
-    gkey[g] = lowered_key(r, low);
-    t.max_lowered = std::max(t.max_lowered, r);
-  }
-  std::vector<size_t> ord(ng);
-  for (size_t g = 0; g < ng; ++g) ord[g] = g;
-  std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return gkey[a] < gkey[b]; });
-  std::vector<Group> sorted(ng);
-  t.seg_key.clear();
-  t.seg_begin.clear();
-  for (size_t i = 0; i < ng; ++i) {
-    const size_t g = ord[i];
-    sorted[i] = t.groups[g];
-    if (t.seg_key.empty() || t.seg_key.back() != gkey[g]) {
-      t.seg_key.push_back(gkey[g]);
-      t.seg_begin.push_back((int)i);
+  index_groups(t, &per_group);
+}
+
+bool build_gate_patterns(const Model& m, ConnTables& t, int64_t max_patterns) {
+  t.groups.clear(); t.terms.clear(); t.diag_terms.clear();
+  const int nm = m.nm;
+  // change vectors with |delta|_1 = s, s even <= fcmax or s odd <= fcmax - 1 (Ham.cpp:247,283);
+  // the number of changed modes is at most s, so the mode-count gates hold by themselves
+  const int smax = m.fcmax;
+  std::vector<int> modes(kMaxOrder), deltas(kMaxOrder);
+  bool over = false;
+  // choose k modes m_1 < .. < m_k and nonzero deltas with sum |d| = s
+  std::function<void(int, int, int, int)> rec = [&](int start, int k, int used, int s) {
+    if (over) return;
+    if (used == s) {
+      if (k == 0) return;
+      Group g;
+      g.nchg = k;
+      for (int a = 0; a < k; ++a) { g.mode[a] = modes[a]; g.delta[a] = deltas[a]; }
+      t.groups.push_back(g);
+      if ((int64_t)t.groups.size() > max_patterns) over = true;
+      return;
     }
-    sorted[i].term_begin = (int)t.terms.size();
-    t.terms.insert(t.terms.end(), per_group[g].begin(), per_group[g].end());
-    sorted[i].term_end = (int)t.terms.size();
+    if (k == kMaxOrder) return;
+    for (int mm = start; mm < nm; ++mm)
+      for (int d = 1; used + d <= s; ++d)
+        for (int sg = -1; sg <= 1; sg += 2) {
+          modes[k] = mm;
+          deltas[k] = sg * d;
+          rec(mm + 1, k + 1, used + d, s);
+          if (over) return;
+        }
+  };
+  for (int s = 1; s <= smax && !over; ++s) {
+    if (s % 2 == 1 && s > smax - 1) continue;
+    rec(0, 0, 0, s);
   }
-  t.seg_begin.push_back((int)ng);
-  t.groups.swap(sorted);
+  if (over) { t.groups.clear(); return false; }
+  index_groups(t, nullptr);
+  return true;
 }
 
 void build_hb_entries(const Model& m, std::vector<HBEntry>& e, std::vector<int64_t>& cum) {

@@ -83,6 +83,10 @@ struct ConnTables {
   int max_lowered = 0;           // most modes one group lowers
 };
 void build_conn_tables(const Model& m, ConnTables& t);
+// Every change vector the reference's pair gates admit (|delta|_1 = s, s even <= fcmax, s odd <=
+// fcmax - 1; Ham.cpp:247,283), as groups without terms, indexed like the connection groups.
+// False (and empty) when there are more than max_patterns.
+bool build_gate_patterns(const Model& m, ConnTables& t, int64_t max_patterns);
 
 // ---- heat-bath pattern descriptors ----
 struct HBEntry {

@@ -1,7 +1,9 @@
 // `vhci` command-line tool: drop-in for the reference's `vhci -n Ncpus -i in.inp -o freqs.dat
 // [-c checkpoint]` (VHCI.cpp:5-185, Input_Reader.cpp:17-168) on top of the C ABI.  stdout carries
 // the reference's messages; handled errors exit with status 0 as the reference does, unless
-// --strict is given (then 1).  Extra flags: --mixed (FP32 Hamiltonian storage), --device N.
+// --strict is given (then 1).  Extra flags: --mixed (FP32 Hamiltonian storage), --device N,
+// --stored-sparsity (the "% sparse" line from the stored nonzero entries instead of the
+// reference's structural pattern count).
 #include <sys/stat.h>
 
 #include <cstdlib>
@@ -75,6 +77,7 @@ int main(int argc, char* argv[]) {
   vhci_opts o;
   vhci_default_opts(&o);
   o.verbose = 1;
+  o.structural_nnz = 1;  // the reference's "% sparse" counts structural zeros too
   std::string inp, outp, cp = "none";
   int ncpus = 0;
   bool have_in = false, have_out = false;
@@ -83,6 +86,7 @@ int main(int argc, char* argv[]) {
     std::string a = argv[i];
     if (a == "--strict") { strict = true; continue; }
     if (a == "--mixed") { o.precision = 1; continue; }
+    if (a == "--stored-sparsity") { o.structural_nnz = 0; continue; }
     if (a == "--device" && i + 1 < argc) { o.device = std::atoi(argv[++i]); continue; }
     args.push_back(a);
   }
