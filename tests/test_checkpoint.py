@@ -92,3 +92,30 @@ def test_checkpoint_validation(api, tmp_path):
             with pytest.raises(api.VhciError) as e:
                 v.read_checkpoint(p)
             assert msg in str(e.value)
+
+
+def test_checkpoint_text_is_byte_identical_to_printf(api, tmp_path):
+    """The parallel writer produces exactly the reference's text: 'N M NEig', then '%.17f '
+    fields (Core_functions.cpp:94-117), checked against Python's correctly rounded formatting;
+    and the parallel reader restores the same basis and vectors."""
+    g = load_golden("syn_m9_eps0_pt2")
+    path = str(tmp_path / "ck.txt")
+    with api.VHCI(g["input"], host_threads=7) as v:
+        v.hci()
+        v.write_checkpoint(path)
+        k = v.info.nstate
+        C, E = v.vectors(k)
+        q = v.basis().astype(int)
+        f = v.freqs()
+    n, nm = q.shape
+    want = [f"{n} {nm} {k}\n", "".join("%.17f " % x for x in f) + "".join("%.17f " % x for x in E) + "\n"]
+    for i in range(n):
+        want.append("".join("%d " % x for x in q[i]) + "".join("%.17f " % x for x in C[i]) + "\n")
+    assert open(path).read() == "".join(want)
+    with api.VHCI(g["input"], restart=True, host_threads=5) as v:
+        v.read_checkpoint(path)
+        C2, E2 = v.vectors(k)
+        assert np.array_equal(v.basis().astype(int), q)
+    C_txt = np.array([[float("%.17f" % x) for x in row] for row in C])
+    assert np.array_equal(C2, C_txt)
+    assert np.array_equal(E2, np.array([float("%.17f" % x) for x in E]))

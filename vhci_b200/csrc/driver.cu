@@ -1,7 +1,13 @@
 // Host orchestration: Epstein-Nesbet PT2 (PT2.cpp:16-154), the heat-bath driver loop
 // (Perform_HCI, HB.cpp:176-265; VHCI.cpp:49-80) and the reference's output and checkpoint files
 // (PrintFreqs, Ham.cpp:448-502; Write/ReadCheckpoint, Core_functions.cpp:94-167).
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -9,6 +15,7 @@
 #include <iomanip>
 #include <iostream>
 #include <sstream>
+#include <thread>
 
 #include "internal.h"
 
@@ -165,6 +172,77 @@ int write_cp(vhci_ctx* c, const char* path) {
   }
   return VHCI_OK;
 }
+
+
+// ---- checkpoint text: "%.17f " fields and integer quanta, formatted and parsed in parallel ----
+
+int host_threads(vhci_ctx* c) {
+  int t = c->o.host_threads > 0 ? c->o.host_threads : (int)std::thread::hardware_concurrency();
+  return std::max(1, std::min(t, 64));
+}
+
+template <class F>
+void parallel_for(int T, F&& f) {
+  if (T <= 1) { f(0); return; }
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) th.emplace_back([&f, t] { f(t); });
+  f(0);
+  for (auto& x : th) x.join();
+}
+
+// Appends the value as printf("%.17f ") prints it: std::to_chars in fixed notation is correctly
+// rounded, as glibc's printf is, so the text is the same.
+void append_fixed17(std::string& b, double v) {
+  char tmp[400];
+  const auto r = std::to_chars(tmp, tmp + sizeof tmp, v, std::chars_format::fixed, 17);
+  b.append(tmp, r.ptr);
+  b += ' ';
+}
+
+inline void skip_space(const char*& p, const char* end) {
+  while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
+}
+
+template <class I>
+bool next_int(const char*& p, const char* end, I& v) {
+  skip_space(p, end);
+  if (p < end && *p == '+') ++p;
+  const auto r = std::from_chars(p, end, v);
+  if (r.ec != std::errc()) return false;
+  p = r.ptr;
+  return true;
+}
+
+bool next_double(const char*& p, const char* end, double& v) {
+  skip_space(p, end);
+  if (p < end && *p == '+') ++p;
+  const auto r = std::from_chars(p, end, v);
+  if (r.ec != std::errc()) return false;
+  p = r.ptr;
+  return true;
+}
+
+// Read-only mapping of a whole file.
+struct MappedFile {
+  const char* data = nullptr;
+  size_t size = 0;
+  int fd = -1;
+  bool open(const char* path) {
+    fd = ::open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size <= 0) return false;
+    size = (size_t)st.st_size;
+    void* m = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (m == MAP_FAILED) { size = 0; return false; }
+    data = (const char*)m;
+    return true;
+  }
+  ~MappedFile() {
+    if (data) munmap((void*)data, size);
+    if (fd >= 0) ::close(fd);
+  }
+};
 
 }  // namespace
 
@@ -336,50 +414,107 @@ vhci_status vhci_write_checkpoint(const vhci_ctx* c0, const char* path) {
   if (nv > 0) VTRY(vhci_get_vectors(c, C.data(), nullptr, nv));
   FILE* f = std::fopen(path, "w");
   if (!f) return fail(c, VHCI_E_INPUT, "checkpoint file could not be opened");
-  std::fprintf(f, "%lld %d %d\n", (long long)n, nm, c->M.nstate);
-  for (int j = 0; j < nm; ++j) std::fprintf(f, "%.17f ", c->M.freq[j]);
-  for (int j = 0; j < nv; ++j) std::fprintf(f, "%.17f ", c->E[j]);
-  std::fprintf(f, "\n");
-  for (int64_t i = 0; i < n; ++i) {
-    for (int j = 0; j < nm; ++j) std::fprintf(f, "%d ", (int)q[(size_t)i * nm + j]);
-    for (int j = 0; j < nv; ++j) std::fprintf(f, "%.17f ", C[(size_t)j * n + i]);
-    std::fprintf(f, "\n");
+  std::string head = std::to_string(n) + " " + std::to_string(nm) + " " + std::to_string(c->M.nstate) + "\n";
+  for (int j = 0; j < nm; ++j) append_fixed17(head, c->M.freq[j]);
+  for (int j = 0; j < nv; ++j) append_fixed17(head, c->E[j]);
+  head += '\n';
+  std::fwrite(head.data(), 1, head.size(), f);
+  // rows formatted in parallel chunks, written in order
+  const int T = host_threads(c);
+  const int64_t rows = std::max<int64_t>(256, (int64_t)(32e6 / (4.0 * nm + 24.0 * nv + 1.0)));
+  std::vector<std::string> buf(T);
+  bool ok = true;
+  for (int64_t r0 = 0; r0 < n && ok; r0 += rows * T) {
+    parallel_for(T, [&](int t) {
+      std::string& b = buf[t];
+      b.clear();
+      const int64_t lo = r0 + t * rows, hi = std::min(n, lo + rows);
+      for (int64_t i = lo; i < hi; ++i) {
+        for (int j = 0; j < nm; ++j) {
+          b += std::to_string((int)q[(size_t)i * nm + j]);
+          b += ' ';
+        }
+        for (int j = 0; j < nv; ++j) append_fixed17(b, C[(size_t)j * n + i]);
+        b += '\n';
+      }
+    });
+    for (int t = 0; t < T && ok; ++t)
+      ok = std::fwrite(buf[t].data(), 1, buf[t].size(), f) == buf[t].size();
   }
-  std::fclose(f);
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(c, VHCI_E_INPUT, "checkpoint file could not be written");
   return VHCI_OK;
 }
 
 // ReadCheckpoint (Core_functions.cpp:119-167): validates the mode count, Nstate and the
-// frequencies (exact equality), then replaces the basis and the vectors.
+// frequencies (exact equality), then replaces the basis and the vectors.  The file is mapped and
+// its rows parsed in parallel.
 vhci_status vhci_read_checkpoint(vhci_ctx* c, const char* path) {
   if (!c || !path) return VHCI_E_INPUT;
-  std::ifstream in(path);
-  if (!in.good()) return fail(c, VHCI_E_INPUT, "checkpoint file could not be opened");
+  MappedFile mf;
+  if (!mf.open(path)) return fail(c, VHCI_E_INPUT, "checkpoint file could not be opened");
+  const char* p = mf.data;
+  const char* end = mf.data + mf.size;
   long long nb = 0;
   int m = 0, ne = 0;
-  in >> nb >> m >> ne;
-  if (!in || nb <= 0) return fail(c, VHCI_E_INPUT, "Error: malformed checkpoint file.");
+  if (!next_int(p, end, nb) || !next_int(p, end, m) || !next_int(p, end, ne) || nb <= 0)
+    return fail(c, VHCI_E_INPUT, "Error: malformed checkpoint file.");
   if (m != c->M.nm) return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong number of fundamental modes!");
   if (ne != c->M.nstate) return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong number of eigenstates!");
   for (int i = 0; i < m; ++i) {
     double f = 0;
-    in >> f;
-    if (f != c->M.freq[i]) return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong fundamental frequencies!");
+    if (!next_double(p, end, f) || f != c->M.freq[i])
+      return fail(c, VHCI_E_INPUT, "Error: Checkpoint file contains wrong fundamental frequencies!");
   }
   std::vector<double> E(ne);
-  for (int i = 0; i < ne; ++i) in >> E[i];
+  for (int i = 0; i < ne; ++i)
+    if (!next_double(p, end, E[i])) return fail(c, VHCI_E_INPUT, "Error: truncated checkpoint file.");
+  // rows: one per line after the header lines; split the rest of the file among the threads at
+  // line starts, count each part's lines, then parse every part into its rows
+  while (p < end && *p != '\n') ++p;
+  if (p < end) ++p;
+  const int T = host_threads(c);
+  std::vector<const char*> cut(T + 1);
+  cut[0] = p;
+  cut[T] = end;
+  for (int t = 1; t < T; ++t) {
+    const char* x = p + (end - p) * t / T;
+    if (x < cut[t - 1]) x = cut[t - 1];
+    while (x < end && x > p && x[-1] != '\n') ++x;
+    cut[t] = x;
+  }
+  std::vector<int64_t> lines(T + 1, 0);
+  parallel_for(T, [&](int t) {
+    int64_t k = 0;
+    for (const char* x = cut[t]; x < cut[t + 1]; ++x) k += *x == '\n';
+    if (cut[t + 1] == end && cut[t + 1] > cut[t] && end[-1] != '\n') ++k;  // last line unterminated
+    lines[t + 1] = k;
+  });
+  for (int t = 0; t < T; ++t) lines[t + 1] += lines[t];
+  if (lines[T] < nb) return fail(c, VHCI_E_INPUT, "Error: truncated checkpoint file.");
   std::vector<uint8_t> q((size_t)nb * m);
   std::vector<double> C((size_t)nb * ne);
-  for (long long i = 0; i < nb; ++i) {
-    for (int j = 0; j < m; ++j) {
-      int qq = 0;
-      in >> qq;
-      if (qq < 0 || qq > 255) return fail(c, VHCI_E_KEY_OVERFLOW, "checkpoint quanta out of range");
-      q[(size_t)i * m + j] = (uint8_t)qq;
+  std::vector<int> bad(T, 0);
+  parallel_for(T, [&](int t) {
+    const char* x = cut[t];
+    const char* e = cut[t + 1];
+    for (int64_t i = lines[t]; i < std::min<int64_t>(lines[t + 1], nb); ++i) {
+      for (int j = 0; j < m; ++j) {
+        long long qq = 0;
+        if (!next_int(x, e, qq)) { bad[t] = 1; return; }
+        if (qq < 0 || qq > 255) { bad[t] = 2; return; }
+        q[(size_t)i * m + j] = (uint8_t)qq;
+      }
+      for (int j = 0; j < ne; ++j)
+        if (!next_double(x, e, C[(size_t)j * nb + i])) { bad[t] = 1; return; }
+      while (x < e && *x != '\n') ++x;
+      if (x < e) ++x;
     }
-    for (int j = 0; j < ne; ++j) in >> C[(size_t)j * nb + i];
+  });
+  for (int t = 0; t < T; ++t) {
+    if (bad[t] == 2) return fail(c, VHCI_E_KEY_OVERFLOW, "checkpoint quanta out of range");
+    if (bad[t]) return fail(c, VHCI_E_INPUT, "Error: truncated checkpoint file.");
   }
-  if (!in) return fail(c, VHCI_E_INPUT, "Error: truncated checkpoint file.");
   VTRY(vhci_set_basis(c, q.data(), nb));
   VTRY(vhci_set_vectors(c, C.data(), E.data(), ne));
   c->restart = 1;
