@@ -193,26 +193,12 @@ def run_ours(args):
     import torch
     from vhci_b200 import api
 
+    from vhci_b200.replicas import Replicas, job_seconds_per_solve
+
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def allmax(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas()            # NCCL process group of the replica ranks (none at N = 1)
+    barrier, allmax = rep.barrier, rep.allmax
 
     td = tempfile.mkdtemp(prefix="vhci_bench_")
     path = os.path.join(td, "workload.inp")
@@ -249,7 +235,7 @@ def run_ours(args):
 
     dev_s = allmax(sum(dev_ms) / 1e3)
     wall_s = allmax(wall)
-    value = dev_s / (args.steps * ws)
+    value = job_seconds_per_solve(dev_s, args.steps, ws)
 
     # end to end through the public call, host inputs and outputs
     barrier()
@@ -262,7 +248,7 @@ def run_ours(args):
         h2d += r["stats"]["h2d_bytes"]
         d2h += r["stats"]["d2h_bytes"]
     barrier()
-    e2e_s = allmax(e2e_t) / (args.steps * ws)
+    e2e_s = job_seconds_per_solve(allmax(e2e_t), args.steps, ws)
 
     hbm, peak_kind = measured_peaks()
     spmm_gbs = st["spmm_bytes"] / (st["ms_spmm"] / 1e3) / 1e9 if st["ms_spmm"] else None
@@ -304,8 +290,7 @@ def run_ours(args):
                        "pairs (H builds + PT2); selection and eigensolver time not included")}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def run_spmm_sweep(args):
