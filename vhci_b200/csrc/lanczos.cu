@@ -181,10 +181,20 @@ int lanczos_block(int64_t n) {
   return 16;
 }
 
+// Guard vectors kept beyond the k wanted pairs at a restart: 60 % of k (at least 8;
+// VHCI_LANCZOS_GUARD=p sets p %).  With subspace 2 kk + 2 b this needed 17-32 % fewer block
+// products than 10 % with 3 kk + 2 b on three workloads (k = 50, 128, 200): keeping more of the
+// Krylov space across restarts pays more than expanding further between them.
+static int lanczos_guard(int k) {
+  int pct = 60;
+  if (const char* e = std::getenv("VHCI_LANCZOS_GUARD")) pct = std::max(1, std::min(200, std::atoi(e)));
+  return std::max(8, k * pct / 100);
+}
+
 // Working set of the block Lanczos for subspace factor `span`: Q and H Q (n x ld), the Ritz block
 // and its product (n x kk), the expansion block and its compact copy (n x b), in doubles.
 static double lanczos_bytes(int64_t n, int k, int span, int b) {
-  const int kk = (int)std::min<int64_t>(n, k + std::max(8, k / 10));
+  const int kk = (int)std::min<int64_t>(n, k + lanczos_guard(k));
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   const int ld = (mmax + b + 15) / 16 * 16;
   return 8.0 * (double)n * (2.0 * ld + 2.0 * kk + 2.0 * b);
@@ -193,7 +203,7 @@ static double lanczos_bytes(int64_t n, int k, int span, int b) {
 // Working set of the memory-lean variant: Q (n x ld, span 2), the expansion block, its product,
 // the compact copy (n x b each), the rotation chunk, and the output Ritz block (n x kk).
 static double lanczos_lean_bytes(int64_t n, int k, int b, int span = 2) {
-  const int kk = (int)std::min<int64_t>(n, k + std::max(8, k / 10));
+  const int kk = (int)std::min<int64_t>(n, k + lanczos_guard(k));
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   const int ld = (mmax + b + 15) / 16 * 16;
   return 8.0 * (double)n * (ld + 3.0 * b + kk) + 2.6e8;
@@ -208,21 +218,17 @@ int block_lanczos_lean(vhci_ctx* c, int k);
 int block_lanczos(vhci_ctx* c, int k) {
   const int64_t n = c->n;
   cudaStream_t s = c->st;
-  const int guard = std::max(8, k / 10);
+  const int guard = lanczos_guard(k);
   const int kk = (int)std::min<int64_t>(n, k + guard);
   const int b = lanczos_block(n);
-  // subspace size: 3 kk + 2 b by default (VHCI_LANCZOS_SPAN overrides the factor 3); a basis too
-  // large for that working set in the free device memory runs with factor 2
-  int span = 3;
+  // subspace size: 2 kk + 2 b (VHCI_LANCZOS_SPAN overrides the factor 2); a basis too large for
+  // that working set in the free device memory runs the memory-lean variant
+  int span = 2;
   const double avail = device_available(c);
   if (const char* e = std::getenv("VHCI_LANCZOS_LEAN"))
     if (std::atoi(e) == 1) return block_lanczos_lean(c, k);
-  if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) {
-    span = std::max(2, std::min(8, std::atoi(e)));
-  } else if (lanczos_bytes(n, k, 3, b) + 1e9 > avail) {
-    span = 2;
-    if (lanczos_bytes(n, k, 2, b) + 1e9 > avail) return block_lanczos_lean(c, k);
-  }
+  if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) span = std::max(2, std::min(8, std::atoi(e)));
+  if (lanczos_bytes(n, k, span, b) + 1e9 > avail) return block_lanczos_lean(c, k);
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
@@ -404,8 +410,7 @@ int block_lanczos(vhci_ctx* c, int k) {
 
 
 // Memory-lean block Lanczos for bases whose Hamiltonian leaves too little device memory for the
-// stored H Q blocks and Ritz blocks: the same thick-restart method (subspace 3 kk + 2 b when it
-// fits, else 2 kk + 2 b), but
+// stored H Q blocks and Ritz blocks: the same thick-restart method (subspace 2 kk + 2 b), but
 //   * only Q is stored; each step's product H Q_new lives in one n x b buffer, from which the new
 //     column of T = Q^T H Q and the next block are formed at once;
 //   * convergence is judged from the Krylov relation H Q = Q T + W E_last^T (W: the pending block,
@@ -416,13 +421,10 @@ int block_lanczos(vhci_ctx* c, int k) {
 int block_lanczos_lean(vhci_ctx* c, int k) {
   const int64_t n = c->n;
   cudaStream_t s = c->st;
-  const int guard = std::max(8, k / 10);
+  const int guard = lanczos_guard(k);
   const int kk = (int)std::min<int64_t>(n, k + guard);
   const int b = lanczos_block(n);
-  // the largest subspace factor (3, else 2) whose lean working set fits; the previous Ritz block
-  // (n_old x kk) is released after the start block is formed, so it counts as available
-  const double avail = device_available(c) + 8.0 * (double)c->x_rows * c->ldx;
-  const int span = lanczos_lean_bytes(n, k, b, 3) + 1e9 <= avail ? 3 : 2;
+  const int span = 2;
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   const int ld = (mmax + b + 15) / 16 * 16;
   const double one = 1.0, zero = 0.0, mone = -1.0;
