@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "internal.h"
 
@@ -78,6 +79,54 @@ static int upload(vhci_ctx* c, DBuf<T>& b, const std::vector<T>& h) {
   if (!h.empty())
     VCK(h2d(c, b.p, h.data(), h.size() * sizeof(T)));
   return VHCI_OK;
+}
+
+// ---- stream and library handles, pooled per device ----------------------------------------
+// Creating cuBLAS and cuSOLVER handles costs tens of milliseconds; a context borrows a set (stream
+// + handles) from its device's pool and returns it, idle, on destroy, so a process that runs many
+// solves creates each set once.  Concurrent contexts hold different sets.  Pooled sets live until
+// the process exits.
+namespace {
+struct HandleSet {
+  int device;
+  cudaStream_t st;
+  cublasHandle_t blas;
+  cusolverDnHandle_t sol;
+};
+std::mutex g_handle_mu;
+std::vector<HandleSet> g_handle_pool;
+}  // namespace
+
+static int acquire_handles(vhci_ctx* c) {
+  {
+    std::lock_guard<std::mutex> lk(g_handle_mu);
+    for (size_t i = 0; i < g_handle_pool.size(); ++i)
+      if (g_handle_pool[i].device == c->o.device) {
+        c->st = g_handle_pool[i].st;
+        c->blas = g_handle_pool[i].blas;
+        c->sol = g_handle_pool[i].sol;
+        g_handle_pool.erase(g_handle_pool.begin() + i);
+        return VHCI_OK;
+      }
+  }
+  VCK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  VBL(cublasCreate(&c->blas));
+  VBL(cublasSetStream(c->blas, c->st));
+  VBL(cusolverDnCreate(&c->sol));
+  VBL(cusolverDnSetStream(c->sol, c->st));
+  return VHCI_OK;
+}
+
+static void release_handles(vhci_ctx* c) {
+  if (!c->st || !c->blas || !c->sol) {  // a partly built set is not pooled
+    if (c->blas) cublasDestroy(c->blas);
+    if (c->sol) cusolverDnDestroy(c->sol);
+    if (c->st) cudaStreamDestroy(c->st);
+    return;
+  }
+  cudaStreamSynchronize(c->st);
+  std::lock_guard<std::mutex> lk(g_handle_mu);
+  g_handle_pool.push_back(HandleSet{c->o.device, c->st, c->blas, c->sol});
 }
 
 // Layout-dependent tables (packed key deltas, ladder factors) and the layout-free ones.
@@ -526,7 +575,6 @@ static int create_common(vhci_ctx* c, int restart) {
     return fail(c, VHCI_E_CUDA, "no CUDA device available (this library has no CPU path)");
   if (c->o.device < 0 || c->o.device >= ndev) return fail(c, VHCI_E_CUDA, "bad device ordinal");
   VCK(cudaSetDevice(c->o.device));
-  VCK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   VCK(cudaEventCreate(&c->ev_a));
   VCK(cudaEventCreate(&c->ev_b));
   {
@@ -536,10 +584,7 @@ static int create_common(vhci_ctx* c, int restart) {
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
   }
-  VBL(cublasCreate(&c->blas));
-  VBL(cublasSetStream(c->blas, c->st));
-  VBL(cusolverDnCreate(&c->sol));
-  VBL(cusolverDnSetStream(c->sol, c->st));
+  VTRY(acquire_handles(c));
   VCK(c->flags.reserve(4, c->st));
   VCK(cudaMemsetAsync(c->flags.p, 0, 4 * sizeof(int), c->st));
   VTRY(upload_tables(c));
@@ -621,13 +666,14 @@ vhci_status vhci_destroy(vhci_ctx* c) {
     c->d64a.release(c->st); c->u64a.release(c->st); c->u64b.release(c->st);
     c->u8a.release(c->st); c->ull.release(c->st); c->solver_work.release(c->st);
     c->solver_info.release(c->st);
+    c->lkey.release(c->st); c->lseg.release(c->st);
+    c->prow.release(c->st); c->pcol.release(c->st); c->pval.release(c->st);
+    c->pvalf.release(c->st); c->gate_dev.release(c->st);
     cudaStreamSynchronize(c->st);
   }
-  if (c->blas) cublasDestroy(c->blas);
-  if (c->sol) cusolverDnDestroy(c->sol);
   if (c->ev_a) cudaEventDestroy(c->ev_a);
   if (c->ev_b) cudaEventDestroy(c->ev_b);
-  if (c->st) cudaStreamDestroy(c->st);
+  release_handles(c);
   delete c;
   return VHCI_OK;
 }
