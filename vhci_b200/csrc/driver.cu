@@ -24,9 +24,9 @@ namespace vhci {
 int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
   if (c->nvec < 1 || c->x_rows != c->n) return fail(c, VHCI_E_STATE, "PT2 needs eigenvectors");
   cudaStream_t s = c->st;
-  cudaEvent_t t0, t1;
-  VCK(cudaEventCreate(&t0));
-  VCK(cudaEventCreate(&t1));
+  EventPair ev_t0t1;
+  VCK(ev_t0t1.create());
+  cudaEvent_t t0 = ev_t0t1.a, t1 = ev_t0t1.b;
   VCK(cudaEventRecord(t0, s));
   const int64_t n = c->n;
   const int nopt = (int)std::min<int64_t>(std::min<int64_t>(c->M.nstate, n), c->nvec);
@@ -102,9 +102,9 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       VCK(h2d(c, crow.p, cr.data(), cr.size() * sizeof(int64_t)));
       VCK(cudaMemsetAsync(acount.p, 0, (a1 - a0) * sizeof(int32_t), s));
       pt2_fill(c->keys.p, n, L, pv, conn_view(c), a0, a1, crow.p, acount.p, ecol.p, eval.p, s);
-      cudaEvent_t r0, r1;
-      VCK(cudaEventCreate(&r0));
-      VCK(cudaEventCreate(&r1));
+      EventPair ev_r0r1;
+      VCK(ev_r0r1.create());
+      cudaEvent_t r0 = ev_r0r1.a, r1 = ev_r0r1.b;
       VCK(cudaEventRecord(r0, s));
       pt2_en(pkeys.p, a0, a1, L, conn_view(c), crow.p, ecol.p, eval.p, c->X.p, c->ldx, nopt,
              Ed.p, part.p, s);
@@ -113,8 +113,6 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       VCK(cudaEventSynchronize(r1));
       float ms = 0.f;
       cudaEventElapsedTime(&ms, r0, r1);
-      cudaEventDestroy(r0);
-      cudaEventDestroy(r1);
       c->stats.ms_pt2_reduce += ms;
       const int64_t ent = cr.back();
       c->stats.pt2_reduce_bytes += ent * (4 + 8) + ent * (int64_t)nopt * 8 + (a1 - a0) * (8 + 8 * L.W);
@@ -136,8 +134,6 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
   VCK(cudaEventSynchronize(t1));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, t0, t1);
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   c->stats.ms_pt2 += ms;
   if (n_pert) *n_pert = np;
   return VHCI_OK;
@@ -252,9 +248,9 @@ vhci_status vhci_hci(vhci_ctx* c, const char* checkpoint_path, vhci_iter_cb cb, 
   if (!c) return VHCI_E_INPUT;
   const bool v = c->o.verbose != 0;
   const int k = c->M.nstate;
-  cudaEvent_t t0, t1;
-  VCK(cudaEventCreate(&t0));
-  VCK(cudaEventCreate(&t1));
+  EventPair ev_t0t1;
+  VCK(ev_t0t1.create());
+  cudaEvent_t t0 = ev_t0t1.a, t1 = ev_t0t1.b;
   VCK(cudaEventRecord(t0, c->st));
   if (c->M.eps1 == 0.0) {  // conventional VCI over the initial basis (VHCI.cpp:49-76)
     if (!c->restart || c->nvec == 0) {
@@ -319,8 +315,6 @@ vhci_status vhci_hci(vhci_ctx* c, const char* checkpoint_path, vhci_iter_cb cb, 
   VCK(cudaEventSynchronize(t1));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, t0, t1);
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   c->stats.ms_total += ms;
   return VHCI_OK;
 }

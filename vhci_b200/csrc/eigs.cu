@@ -137,9 +137,9 @@ int project_out(vhci_ctx* c, Work& w, int64_t n, const double* V, int ldv, int m
 }
 
 int apply_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
-  cudaEvent_t e0, e1;
-  VCK(cudaEventCreate(&e0));
-  VCK(cudaEventCreate(&e1));
+  EventPair ev_e0e1;
+  VCK(ev_e0e1.create());
+  cudaEvent_t e0 = ev_e0e1.a, e1 = ev_e0e1.b;
   VCK(cudaEventRecord(e0, c->st));
   spmm_h(c, X, ldx, b, Y, ldy);
   VCK(cudaEventRecord(e1, c->st));
@@ -147,8 +147,6 @@ int apply_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
   VCK(cudaGetLastError());
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   c->stats.ms_spmm += ms;
   c->stats.spmm_calls += 1;
   c->stats.spmm_cols += b;

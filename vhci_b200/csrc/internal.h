@@ -43,6 +43,19 @@ int append_keys(vhci_ctx* c, const uint64_t* dkeys, int64_t m);
 int generate_new_set(vhci_ctx* c, double eps);
 
 int build_h(vhci_ctx* c);
+// Two CUDA events that are destroyed with their scope, so early error returns release them.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t create() {
+    cudaError_t e = cudaEventCreate(&a);
+    return e == cudaSuccess ? cudaEventCreate(&b) : e;
+  }
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 // Entries of the reference's stored pattern (diagonal + gated pairs, structural zeros included).
 bool structural_available(vhci_ctx* c);
 int structural_count(vhci_ctx* c, int64_t* out);

@@ -146,9 +146,9 @@ int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb
 // Y = H X for a block: X is first copied to a compact n x b buffer so the SpMM gathers from a
 // small, L2-resident array instead of rows of the wide basis.
 int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y, int ldy) {
-  cudaEvent_t e0, e1;
-  VCK(cudaEventCreate(&e0));
-  VCK(cudaEventCreate(&e1));
+  EventPair ev_e0e1;
+  VCK(ev_e0e1.create());
+  cudaEvent_t e0 = ev_e0e1.a, e1 = ev_e0e1.b;
   VCK(w.Xc.reserve((size_t)c->n * b, c->st));
   VCK(cudaEventRecord(e0, c->st));
   copy_cols(X, ldx, w.Xc.p, b, c->n, b, c->st);
@@ -158,8 +158,6 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
   VCK(cudaGetLastError());
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   c->stats.ms_spmm += ms;
   c->stats.spmm_calls += 1;
   c->stats.spmm_cols += b;
