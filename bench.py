@@ -259,7 +259,13 @@ def run_ours(args):
             "peak": hbm, "unit": "GB/s", "frac": (spmm_gbs / hbm) if spmm_gbs else None,
             "traffic": args.traffic if args.traffic else NCU_SPMM_TRAFFIC_PER_LAUNCH,
             "algorithmic_bytes_per_launch": alg_per_launch, "peak_kind": peak_kind,
-            "other": {"k_pt2_en GB/s": en_gbs}}
+            "other": {"k_pt2_en GB/s": en_gbs,
+                      # the product's bound: each of the nnz entries gathers one b-column vector
+                      # row (b * 8 bytes), mostly served from L2
+                      "spmm_gathered_bytes_per_launch": (st["spmm_gather_bytes"] / st["spmm_calls"]
+                                                         if st["spmm_calls"] else None),
+                      "spmm_gather GB/s": (st["spmm_gather_bytes"] / (st["ms_spmm"] / 1e3) / 1e9
+                                           if st["ms_spmm"] else None)}}
 
     line = {
         "metric": "s/solve", "value": value, "unit": "s/solve", "n_gpus": ws,

@@ -102,7 +102,8 @@ class Stats(ctypes.Structure):
                 ("pt2_perturbers", ctypes.c_int64), ("ms_pt2_reduce", ctypes.c_double),
                 ("pt2_reduce_bytes", ctypes.c_int64), ("eig_iterations", ctypes.c_int),
                 ("hci_iterations", ctypes.c_int), ("h2d_bytes", ctypes.c_int64),
-                ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int64)]
+                ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("spmm_gather_bytes", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -151,6 +151,7 @@ int apply_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
   c->stats.spmm_calls += 1;
   c->stats.spmm_cols += b;
   const int64_t sval = c->o.precision == 1 ? 4 : 8;
+  c->stats.spmm_gather_bytes += c->nnz * (int64_t)b * 8;
   c->stats.spmm_bytes += c->nnz * (sval + 4) + (c->n + 1) * 8 + c->n * 8 +
                          2 * c->n * (int64_t)b * 8;
   return VHCI_OK;
