@@ -250,3 +250,24 @@ def test_structural_count_matches_oracle_pair_loop(api, case):
         v.set_basis(o.basis())
         got = v.structural_nnz()
     assert got == int(O.lib().orc_build_h_pairs(o.h))
+
+
+def test_panelled_product_mixed_precision(monkeypatch):
+    """Column panels with FP32 values (mixed precision): the product equals the single-pass FP32
+    product."""
+    from vhci_b200 import api
+    g = load_golden("syn_m8_sextic_pt2")
+    monkeypatch.setenv("VHCI_PANELS", "0")
+    with api.VHCI(g["input"], precision=1) as v:
+        v.hci()
+        X = np.random.default_rng(5).standard_normal((v.n, 16))
+        Y0 = v.apply_h(X)
+        E0 = v.energies().copy()
+    monkeypatch.delenv("VHCI_PANELS")
+    monkeypatch.setenv("VHCI_PANEL_MB", "0.03")
+    with api.VHCI(g["input"], precision=1) as v:
+        v.hci()
+        Y1 = v.apply_h(X)
+        E1 = v.energies().copy()
+    assert np.allclose(Y1, Y0, rtol=1e-13, atol=1e-9)
+    assert np.abs(E1 - E0).max() < 1e-8
