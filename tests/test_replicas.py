@@ -32,7 +32,7 @@ def _rank_main(rank, world, port, out):
 
 def test_two_gloo_ranks_max_and_job_value():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
