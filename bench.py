@@ -120,7 +120,7 @@ def measured_peaks():
 
 def write_workload(path: str) -> None:
     from vhci_b200 import pes
-    pes.write_config(path, WORKLOAD)
+    pes.write_workload(path, WORKLOAD)
 
 
 # ------------------------------------------------------------------------------ reference arm

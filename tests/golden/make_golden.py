@@ -50,7 +50,7 @@ CASES = {
     "clo2_vhci_pt2": _example("CLO2", "VHCI+PT2", "CLO2.inp"),
     "acetonitrile_vhci": _example("Acetonitrile", "VHCI", "acetonitrile.inp"),
     # seeded synthetic PESs
-    "workload0": _synthetic(P.CONFIGS[0][0], P.CONFIGS[0][1], P.config_seed(0)),
+    "workload0": _synthetic(P.WORKLOADS[0][0], P.WORKLOADS[0][1], P.base_seed(0)),
     "syn_m6_pt2": _synthetic(P.PESSpec(6), P.RunSettings(0.5, 20, 1, 0.05), 101),
     "syn_m8_sextic_pt2": _synthetic(P.PESSpec(8, p5=0.05, p6=0.2), P.RunSettings(1.0, 15, 1, 0.1),
                                     102),
@@ -58,8 +58,8 @@ CASES = {
     "syn_m10_vci_pt2": _synthetic(P.PESSpec(10), P.RunSettings(0.0, 20, 1, 0.5, ntot=3), 104),
     "syn_m9_eps0_pt2": _synthetic(P.PESSpec(9), P.RunSettings(2.0, 12, 1, 0.0), 105),
     "syn_m12_pt2": _synthetic(P.PESSpec(12), P.RunSettings(2.0, 30, 1, 0.2), 106),
-    "workload1_small": _synthetic(P.CONFIGS[1][0], P.RunSettings(3.0, 50, 1, 0.3),
-                                  P.config_seed(1)),
+    "workload1_small": _synthetic(P.WORKLOADS[1][0], P.RunSettings(3.0, 50, 1, 0.3),
+                                  P.base_seed(1)),
 }
 
 

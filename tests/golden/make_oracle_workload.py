@@ -30,7 +30,7 @@ def main(workload: int) -> None:
     out = os.path.join(HERE, f"workload{workload}_oracle.json")
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "workload.inp")
-        P.write_config(path, workload)
+        P.write_workload(path, workload)
         t0 = time.time()
         o = O.Oracle(path)
         w, C = np.linalg.eigh(o.dense_h())

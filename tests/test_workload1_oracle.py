@@ -21,7 +21,7 @@ def test_workload1_full_size_matches_oracle(tmp_path):
     from vhci_b200 import api, pes
     ref = json.load(open(FIXTURE))
     path = str(tmp_path / "w1.inp")
-    pes.write_config(path, 1)
+    pes.write_workload(path, 1)
     sizes = []
     with api.VHCI(path) as v:
         v.hci(callback=lambda it, n, zpe: sizes.append(n))

@@ -35,7 +35,7 @@ therefore uses the first draw, over seeds base + 100*j (j = 0, 1, ...), whose po
 non-negative on every one- and two-mode plane within |q| <= sqrt(2*16+1) and on every three-mode
 cube within |q| <= sqrt(2*12+1) (dimensionless normal coordinates, V = sum w q^2/2 +
 sum phi/prod(p_k!) prod q^p_k, i.e. the region spanned by up to 16 resp. 12 quanta per mode).
-`admissible()` implements the test and `CONFIG_SEED_OFFSET` records the first accepted j.
+`admissible()` implements the test and `WORKLOAD_SEED_OFFSET` records the first accepted j.
 """
 from __future__ import annotations
 
@@ -128,7 +128,7 @@ def write_input(path: str, pes: PES, run: RunSettings, comment: str = "synthetic
 
 
 # Benchmark workloads (mode counts, keep probabilities, value ranges and run settings).
-CONFIGS = {
+WORKLOADS = {
     0: (PESSpec(12), RunSettings(eps1=1.0, nstate=50, pt2=0, eps2=0.0)),
     1: (PESSpec(15), RunSettings(eps1=0.5, nstate=200, pt2=1, eps2=0.01)),
     2: (PESSpec(48, p3=0.15, p4=0.02), RunSettings(eps1=1.0, nstate=128, pt2=1, eps2=0.2)),
@@ -138,15 +138,15 @@ CONFIGS = {
 
 
 # First admissible draw j (seed = base + 100*j) per workload, found with `find_admissible`.
-CONFIG_SEED_OFFSET = {0: 0, 1: 1, 2: 39, 4: 6}
+WORKLOAD_SEED_OFFSET = {0: 0, 1: 1, 2: 39, 4: 6}
 
 
-def config_seed(config: int, request: int = 0) -> int:
-    return SEED_BASE + config * 1000 + request
+def base_seed(workload: int, request: int = 0) -> int:
+    return SEED_BASE + workload * 1000 + request
 
 
-def workload_seed(config: int) -> int:
-    return config_seed(config) + 100 * CONFIG_SEED_OFFSET.get(config, 0)
+def workload_seed(workload: int) -> int:
+    return base_seed(workload) + 100 * WORKLOAD_SEED_OFFSET.get(workload, 0)
 
 
 def _subset_terms(pes: PES):
@@ -195,31 +195,31 @@ def admissible(pes: PES, pair_quanta: int = 16, triple_quanta: int = 12) -> bool
     return True
 
 
-def find_admissible(config: int, max_tries: int = 50) -> int:
-    spec, _ = CONFIGS[config]
+def find_admissible(workload: int, max_tries: int = 50) -> int:
+    spec, _ = WORKLOADS[workload]
     for j in range(max_tries):
-        if admissible(generate(spec, config_seed(config) + 100 * j)):
+        if admissible(generate(spec, base_seed(workload) + 100 * j)):
             return j
-    raise RuntimeError(f"no admissible draw for workload {config} in {max_tries} tries")
+    raise RuntimeError(f"no admissible draw for workload {workload} in {max_tries} tries")
 
 
-def write_config(path: str, config: int, run: RunSettings | None = None) -> None:
-    spec, default_run = CONFIGS[config]
-    pes = generate(spec, workload_seed(config))
-    write_input(path, pes, run or default_run, comment=f"synthetic PES, workload {config}")
+def write_workload(path: str, workload: int, run: RunSettings | None = None) -> None:
+    spec, default_run = WORKLOADS[workload]
+    pes = generate(spec, workload_seed(workload))
+    write_input(path, pes, run or default_run, comment=f"synthetic PES, workload {workload}")
 
 
 def serving_request(request: int):
     """One request of the mixed serving stream: Nm in {6..24}, Nstate in {10..100}, eps1 log-uniform
     in [0.3, 3], PT2 on with eps2 = 0.1 * eps1.  The settings come from the request's own stream;
     the PES is redrawn (seed + 100000 j) until it passes `admissible`.  Returns (PES, RunSettings)."""
-    rng = np.random.Generator(np.random.PCG64(config_seed(3, request) + 500))
+    rng = np.random.Generator(np.random.PCG64(base_seed(3, request) + 500))
     nm = int(rng.integers(6, 25))
     nstate = int(rng.integers(10, 101))
     eps1 = float("%.6f" % math.exp(rng.uniform(math.log(0.3), math.log(3.0))))
     eps2 = float("%.6f" % (0.1 * eps1))
     for j in range(200):
-        pes = generate(PESSpec(nm), config_seed(3, request) + 100000 * j)
+        pes = generate(PESSpec(nm), base_seed(3, request) + 100000 * j)
         if admissible(pes):
             return pes, RunSettings(eps1=eps1, nstate=nstate, pt2=1, eps2=eps2)
     raise RuntimeError(f"no admissible PES for serving request {request}")
