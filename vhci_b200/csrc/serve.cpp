@@ -130,13 +130,16 @@ void worker_loop(Server& S, int worker) {
       }
     }
     S.res[r].retries = 0;
+    int solo_done = -1;  // S.done when this request last retried while all others were waiting
     for (;;) {
       solve_one(S, r, worker);
       if (S.res[r].status != VHCI_E_OOM) break;
       // out of device memory (its buffers are already released): wait until another request
-      // finishes; when every running request is waiting, the lowest-numbered one retries
+      // finishes; when every running request is waiting, the lowest-numbered one retries once,
+      // and fails if that retry runs out of memory too with nothing finished in between
       std::unique_lock<std::mutex> lk(S.mu);
-      if (S.running == 1) break;  // alone and still out of memory: report the failure
+      if (S.running == 1) break;        // alone and still out of memory: report the failure
+      if (solo_done == S.done) break;   // its solo retry failed as well: free the slot
       ++S.res[r].retries;
       const int done_before = S.done;
       S.oom_waiting.insert(r);
@@ -145,6 +148,7 @@ void worker_loop(Server& S, int worker) {
         return S.done > done_before ||
                ((int)S.oom_waiting.size() == S.running && *S.oom_waiting.begin() == r);
       });
+      solo_done = S.done > done_before ? -1 : S.done;
       S.oom_waiting.erase(r);
     }
     {
