@@ -421,6 +421,35 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_mixed_check(args):
+    """Mixed precision (FP32 Hamiltonian values, FP64 accumulation, FP64 orthogonalisation, Ritz
+    values and PT2 denominators) against the FP64 path on one workload: device time of each (second
+    of two solves), basis and perturber counts, and the per-state error of the variational and
+    PT2-corrected energies."""
+    import numpy as np
+    from vhci_b200 import api, pes
+    td = tempfile.mkdtemp(prefix="vhci_mixed_")
+    path = os.path.join(td, "workload.inp")
+    pes.write_workload(path, args.workload)
+    res = {}
+    for prec in (0, 1, 0, 1):
+        r = api.solve(path, precision=prec)
+        s = r["stats"]
+        res[prec] = (r, (s["ms_total"] + s["ms_pt2"]) / 1e3)
+    (a, ta), (b, tb) = res[0], res[1]
+    k = min(len(a["E"]), len(b["E"]))
+    line = {
+        "metric": "mixed_vs_fp64", "workload": args.workload,
+        "fp64_s": round(ta, 3), "mixed_s": round(tb, 3), "speedup": round(ta / tb, 3),
+        "n_basis": [a["n_basis"], b["n_basis"]], "n_pert": [a["n_pert"], b["n_pert"]],
+        "max_abs_dE_variational_cm1": float(np.abs(a["E_var"][:k] - b["E_var"][:k]).max()),
+        "max_abs_dE_cm1": float(np.abs(a["E"][:k] - b["E"][:k]).max()),
+        "per_state_abs_dE_cm1": [float(x) for x in np.abs(a["E"][:k] - b["E"][:k])],
+        "target_cm1": 0.01,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -442,12 +471,18 @@ def main():
     ap.add_argument("--max-basis", type=int, default=500_000)
     ap.add_argument("--max-pert", type=int, default=100_000_000)
     ap.add_argument("--verbose-requests", action="store_true")
+    ap.add_argument("--mixed-check", action="store_true",
+                    help="solve a workload in FP64 and in mixed precision, report per-state errors")
+    ap.add_argument("--workload", type=int, default=WORKLOAD)
     args = ap.parse_args()
     if args.spmm_sweep:
         run_spmm_sweep(args)
         return
     if args.serving:
         run_serving(args)
+        return
+    if args.mixed_check:
+        run_mixed_check(args)
         return
     if args.impl == "reference":
         run_reference(args)
