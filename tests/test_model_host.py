@@ -92,3 +92,46 @@ def test_gate_patterns_are_the_admitted_change_vectors(shim, case):
     walk(0, fcmax, [])
     assert len(got) == len(set(got)) and set(got) == want
     _check_segments(shim, got)
+
+
+def test_subset_walk_visits_exactly_the_applicable_groups(shim):
+    """The device enumerator's walk (for_each_group in csrc/conn.cuh), restated: subsets of a
+    state's excited modes of size 0..max lowered, unranked in the combinatorial number system, each
+    looked up by its lowered-mode key in the segment index. It must visit every group whose lowered
+    modes are all excited, once, and nothing else."""
+    from math import comb
+    import numpy as np
+    assert shim.shim_load(load_golden("syn_m8_sextic_pt2")["input"].encode(), 0, 0) == 0
+    nm = shim.shim_nm()
+    groups = _groups(shim)
+    seg = {shim.shim_seg_key(s): (shim.shim_seg_begin(s), shim.shim_seg_begin(s + 1))
+           for s in range(shim.shim_nseg())}
+    maxl = shim.shim_max_lowered()
+    rng = np.random.default_rng(7)
+    for _ in range(200):
+        q = np.zeros(nm, int)
+        k = int(rng.integers(0, nm + 1))
+        q[rng.choice(nm, k, replace=False)] = rng.integers(1, 4, k)
+        exc = [m for m in range(nm) if q[m] > 0]
+        e = len(exc)
+        nsub = sum(comb(e, r) for r in range(min(maxl, e) + 1))
+        seen = []
+        for s in range(nsub):
+            r, rem = 0, s
+            while rem >= comb(e, r):
+                rem -= comb(e, r)
+                r += 1
+            modes, hi = [0] * r, e
+            for i in range(r, 0, -1):        # largest c < hi with C(c, i) <= rem
+                c = hi - 1
+                while comb(c, i) > rem:
+                    c -= 1
+                rem -= comb(c, i)
+                modes[i - 1] = exc[c]
+                hi = c
+            arr = (ctypes.c_int * max(1, r))(*modes)
+            key = shim.shim_lowered_key(r, arr)
+            if key in seg:
+                seen.extend(range(*seg[key]))
+        want = [u for u, g in enumerate(groups) if all(q[m] > 0 for m, d in g if d < 0)]
+        assert len(seen) == len(set(seen)) and sorted(seen) == want
