@@ -179,8 +179,16 @@ vhci_status vhci_residual_norms(vhci_ctx* c, const double* X, const double* thet
  * process exits.  Limits and rules:
  *  - 1 <= k <= 256, else VHCI_E_INPUT;
  *  - the Hamiltonian must already be built (vhci_build_h), else VHCI_E_STATE;
+ *  - X_dev, theta_dev and rnorm_dev must be device memory of the context's device (checked with
+ *    cudaPointerGetAttributes, else VHCI_E_INPUT);
+ *  - the work runs on the context's own stream, which does not wait for the caller's streams:
+ *    the inputs must be complete when the call is made (e.g. synchronise the stream that wrote
+ *    them first);
+ *  - the caller's current device is left as it was;
  *  - the first call on a device looks up the scratch array's device address (and may load the
- *    library's device code); make that first call before any stream capture;
+ *    library's device code); make that first call before any stream capture.  The address is
+ *    kept for the life of the process: after a cudaDeviceReset of that device neither it nor any
+ *    context created before the reset may be used;
  *  - all calls share the one array: calls whose work overlaps on the GPU (from several threads or
  *    contexts on one device) race and must be serialised by the caller. */
 vhci_status vhci_residual_norms_noalloc(vhci_ctx* c, const double* X_dev, const double* theta_dev,

@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ by running the reference VHCI program.
 
-This script runs only in the development container, where the reference tree (with its shipped
-`vhci` executable) is mounted at /root/reference.  The executable is run as a black box in a
-scratch directory (`vhci -n <threads> -i case.inp -o freqs.dat`); its frequency file and the numbers
+This script runs only where the reference tree (with its shipped `vhci` executable) is present;
+its location is given with --reference PATH or the VHCI_REFERENCE environment variable.  The
+executable is run as a black box in a scratch directory (`vhci -n <threads> -i case.inp -o freqs.dat`); its frequency file and the numbers
 printed in its log are stored per case:
 
     tests/golden/<case>/input.inp    the input file (reference example or seeded synthetic PES)
@@ -10,9 +10,9 @@ printed in its log are stored per case:
     tests/golden/<case>/log.json     basis size after each HCI iteration, perturber count,
                                      "% sparse" per Hamiltonian build, ZPE and wall time
 
-The tests read these files only; they never need /root/reference.
+The tests read these files only; they never need the reference tree.
 
-Usage:  python tests/golden/make_golden.py [case ...]
+Usage:  python tests/golden/make_golden.py --reference PATH [case ...]
 """
 from __future__ import annotations
 
@@ -31,12 +31,13 @@ sys.path.insert(0, ROOT)
 
 from vhci_b200 import pes as P  # noqa: E402
 
-REF = "/root/reference"
-BIN = os.path.join(REF, "vhci")
+# location of the reference tree; set from --reference / VHCI_REFERENCE in main
+REF = os.environ.get("VHCI_REFERENCE", "")
+BIN = ""
 
 
 def _example(mol, method, fname):
-    return ("file", os.path.join(REF, "examples", mol, method, fname))
+    return ("file", os.path.join("examples", mol, method, fname))
 
 
 def _synthetic(spec, run, seed):
@@ -85,7 +86,7 @@ def run_case(name: str, threads: int = 8) -> None:
     os.makedirs(out, exist_ok=True)
     inp = os.path.join(out, "input.inp")
     if spec[0] == "file":
-        shutil.copyfile(spec[1], inp)
+        shutil.copyfile(os.path.join(REF, spec[1]), inp)
     else:
         _, pspec, run, seed = spec
         P.write_input(inp, P.generate(pspec, seed), run, comment=f"synthetic PES seed {seed}")
@@ -106,6 +107,14 @@ def run_case(name: str, threads: int = 8) -> None:
 
 
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES)
-    for n in names:
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=REF, help="reference tree (default: $VHCI_REFERENCE)")
+    ap.add_argument("cases", nargs="*")
+    a = ap.parse_args()
+    if not a.reference:
+        sys.exit("give the reference tree with --reference PATH or VHCI_REFERENCE")
+    REF = a.reference
+    BIN = os.path.join(REF, "vhci")
+    for n in a.cases or list(CASES):
         run_case(n)

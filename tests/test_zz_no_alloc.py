@@ -30,9 +30,16 @@ def test_residual_norms_noalloc_matches_allocating_call():
         thd = torch.tensor(th, dtype=torch.float64, device="cuda")
         for _ in range(2):  # two calls in a row share (and reuse) the fixed scratch array
             rd = torch.full((k,), float("nan"), dtype=torch.float64, device="cuda")
+            # the library's stream does not wait for torch's: the inputs must be complete first
+            torch.cuda.synchronize()
             v.residual_norms_noalloc(Xd.data_ptr(), thd.data_ptr(), rd.data_ptr(), k)
             got = rd.cpu().numpy()
             assert np.allclose(got, ref, rtol=1e-12, atol=0), np.abs(got - ref).max()
         with pytest.raises(api.VhciError) as e:  # beyond the fixed array: a clear refusal
             v.residual_norms_noalloc(Xd.data_ptr(), thd.data_ptr(), rd.data_ptr(), 257)
         assert e.value.code == api.E_INPUT
+        host = np.zeros(k)  # a host buffer is refused before anything runs on the device
+        with pytest.raises(api.VhciError) as e:
+            v.residual_norms_noalloc(Xd.data_ptr(), thd.data_ptr(), host.ctypes.data, k)
+        assert e.value.code == api.E_INPUT
+        assert torch.cuda.current_device() == 0

@@ -67,7 +67,8 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     // chunk the perturber range so one chunk's entries fit the budget
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
-    int64_t budget = c->o.pt2_chunk > 0 ? c->o.pt2_chunk : (int64_t)(freeb * 0.6 / 12.0);
+    // entries (12 bytes) plus, in the worst case, the same again as scratch for long-row ordering
+    int64_t budget = c->o.pt2_chunk > 0 ? c->o.pt2_chunk : (int64_t)(freeb * 0.4 / 12.0);
     budget = std::max<int64_t>(budget, 1 << 20);
     std::vector<int64_t> bounds{0};
     while (bounds.back() < np) {
@@ -89,11 +90,14 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     VCK(eval.reserve(std::max<int64_t>(maxchunk, 1), s));
     const int nblk = pt2_en_blocks();
     VCK(part.reserve((size_t)nblk * nopt, s));
+    VCK(cudaMemsetAsync(part.p, 0, (size_t)nblk * nopt * sizeof(double), s));
     VCK(dEd.reserve(nopt, s));
     VCK(Ed.reserve(nopt, s));
     VCK(cudaMemsetAsync(dEd.p, 0, nopt * sizeof(double), s));
     VCK(h2d(c, Ed.p, c->E.data(), nopt * sizeof(double)));
-    DBuf<int64_t> crow;
+    DBuf<int64_t> crow, lrow_d, loff_d;
+    DBuf<int32_t> lcol;
+    DBuf<double> lval;
     for (size_t q = 1; q < bounds.size(); ++q) {
       const int64_t a0 = bounds[q - 1], a1 = bounds[q];
       VCK(crow.reserve(a1 - a0 + 1, s));
@@ -102,12 +106,34 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       VCK(h2d(c, crow.p, cr.data(), cr.size() * sizeof(int64_t)));
       VCK(cudaMemsetAsync(acount.p, 0, (a1 - a0) * sizeof(int32_t), s));
       pt2_fill(c->keys.p, n, L, pv, conn_view(c), a0, a1, crow.p, acount.p, ecol.p, eval.p, s);
+      // fixed entry order per row (the fill's atomics leave it arbitrary): short rows by one warp
+      // each, long rows (listed here from the host copy of the row offsets) by one block each
+      pt2_sort_rows(crow.p, a1 - a0, ecol.p, eval.p, s);
+      std::vector<int64_t> lrows, loff;
+      int64_t ltot = 0;
+      for (int64_t a = a0; a < a1; ++a) {
+        const int64_t len = cr[a - a0 + 1] - cr[a - a0];
+        if (len >= pt2_sort_long_min()) { lrows.push_back(a - a0); loff.push_back(ltot); ltot += len; }
+      }
+      if (!lrows.empty()) {
+        VCK(lrow_d.reserve(lrows.size(), s));
+        VCK(loff_d.reserve(loff.size(), s));
+        VCK(lcol.reserve(ltot, s));
+        VCK(lval.reserve(ltot, s));
+        VCK(h2d(c, lrow_d.p, lrows.data(), lrows.size() * sizeof(int64_t)));
+        VCK(h2d(c, loff_d.p, loff.data(), loff.size() * sizeof(int64_t)));
+        for (size_t q0 = 0; q0 < lrows.size(); q0 += 65535)
+          pt2_sort_long(crow.p, lrow_d.p + q0, loff_d.p + q0,
+                        (int)std::min<size_t>(65535, lrows.size() - q0), ecol.p, eval.p, lcol.p,
+                        lval.p, s);
+      }
       EventPair ev_r0r1;
       VCK(ev_r0r1.create());
       cudaEvent_t r0 = ev_r0r1.a, r1 = ev_r0r1.b;
       VCK(cudaEventRecord(r0, s));
-      pt2_en(pkeys.p, a0, a1, L, conn_view(c), crow.p, ecol.p, eval.p, c->X.p, c->ldx, nopt,
-             Ed.p, part.p, s);
+      if (!pt2_en(pkeys.p, a0, a1, L, conn_view(c), crow.p, ecol.p, eval.p, c->X.p, c->ldx, nopt,
+                  Ed.p, part.p, s))
+        return fail(c, VHCI_E_INPUT, "PT2: unsupported key width or state count");
       VCK(cudaEventRecord(r1, s));
       reduce_parts(part.p, nblk, nopt, dEd.p, s);
       VCK(cudaEventSynchronize(r1));
@@ -125,6 +151,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     if (fl & kFlagTableFull) return fail(c, VHCI_E_TABLE_FULL, "perturber hash full");
     pkeys.release(s); pslots.release(s); acount.release(s); arow.release(s); tmp.release(s);
     ecol.release(s); eval.release(s); part.release(s); dEd.release(s); Ed.release(s); crow.release(s);
+    lrow_d.release(s); loff_d.release(s); lcol.release(s); lval.release(s);
   }
   for (int j = 0; j < nopt; ++j) {
     c->E[j] += dE[j];

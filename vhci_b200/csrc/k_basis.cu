@@ -365,8 +365,10 @@ void select_generate(const uint64_t* keys, int64_t n, const int64_t* woff, int64
 void newset_compact(const uint64_t* cand, const uint8_t* dead, int64_t ncand, int W,
                     uint64_t* out, unsigned long long* n_out, cudaStream_t s) {
   cudaMemsetAsync(n_out, 0, sizeof(unsigned long long), s);
-  if (ncand > 0)
-    note_launch(); k_compact<<<grid_for(ncand, 256), 256, 0, s>>>(cand, dead, ncand, W, out, n_out);
+  if (ncand > 0) {
+    note_launch();
+    k_compact<<<grid_for(ncand, 256), 256, 0, s>>>(cand, dead, ncand, W, out, n_out);
+  }
 }
 
 // ------------------------------------------------------------------------------- radix sort ---

@@ -153,10 +153,21 @@ void pt2_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnD
               double* eval, cudaStream_t s);
 // Fused EN reduction over perturbers [a_lo, a_hi): num_a = sum_e eval_e X[ecol_e, :nopt];
 // E_a = harmonic + diagonal terms; part[blk][n] += num^2 / (E_n - E_a).
+// Every block writes all nopt columns of its part row; any nopt >= 1 (column tiles of 256);
+// returns false for an unsupported key width or nopt < 1 (nothing launched).
 int pt2_en_blocks();
-void pt2_en(const uint64_t* pkeys, int64_t a_lo, int64_t a_hi, KeyLayout L, ConnDev cd,
+bool pt2_en(const uint64_t* pkeys, int64_t a_lo, int64_t a_hi, KeyLayout L, ConnDev cd,
             const int64_t* arowptr, const int32_t* ecol, const double* eval, const double* X,
             int ldx, int nopt, const double* E, double* part, cudaStream_t s);
+// Orders the entries of each perturber row [arowptr[r], arowptr[r+1]) by ascending state index,
+// so the EN sums run in one fixed order.  pt2_sort_rows handles rows shorter than
+// pt2_sort_long_min() entries; pt2_sort_long the listed longer rows (rows[q], with scratch
+// tcol/tval of their total length, row q's part at soff[q]).
+void pt2_sort_rows(const int64_t* arowptr, int64_t nrows, int32_t* ecol, double* eval,
+                   cudaStream_t s);
+int pt2_sort_long_min();
+void pt2_sort_long(const int64_t* arowptr, const int64_t* rows, const int64_t* soff, int nlong,
+                   int32_t* ecol, double* eval, int32_t* tcol, double* tval, cudaStream_t s);
 void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cudaStream_t s);
 
 }  // namespace vhci

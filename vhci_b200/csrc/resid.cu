@@ -142,6 +142,26 @@ __device__ __align__(256) double g_resid_scratch[kResidBlocks * kNoAllocMaxCols]
 std::mutex g_scratch_mu;
 double* g_scratch_dev[128] = {nullptr};  // device address of g_resid_scratch per device ordinal
 
+// Restores the calling thread's current device on every return path.
+struct DeviceGuard {
+  int prev = -1;
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// True when p is device (or managed) memory that device `dev` can address.  Asks the runtime
+// about the pointer; nothing is allocated.
+bool device_pointer_on(const void* p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the (non-sticky) error an unknown pointer may leave
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 }  // namespace
 
 extern "C" vhci_status vhci_residual_norms_noalloc(vhci_ctx* c, const double* X_dev,
@@ -158,7 +178,14 @@ extern "C" vhci_status vhci_residual_norms_noalloc(vhci_ctx* c, const double* X_
                 "first (building it allocates, this call does not)");
   const int dev = c->o.device;
   if (dev < 0 || dev >= 128) return fail(c, VHCI_E_CUDA, "device ordinal out of range");
+  DeviceGuard guard;
+  VCK(cudaGetDevice(&guard.prev));
   VCK(cudaSetDevice(dev));
+  if (!device_pointer_on(X_dev, dev) || !device_pointer_on(theta_dev, dev) ||
+      !device_pointer_on(rnorm_dev, dev))
+    return fail(c, VHCI_E_INPUT,
+                "vhci_residual_norms_noalloc: X_dev, theta_dev and rnorm_dev must be device "
+                "memory of the context's device");
   double* scratch = nullptr;
   {
     // set-up, once per device with that device current: host code only has a host-side stand-in
