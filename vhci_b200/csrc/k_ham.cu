@@ -411,69 +411,6 @@ __global__ void k_sum_parts(const double* __restrict__ part, int nblk, int kk,
   }
 }
 
-__device__ __forceinline__ double precond_den(double th, double d) {
-  double den = th - d;
-  const double g = 1e-6 * fmax(1.0, fabs(th));
-  if (fabs(den) < g) den = den < 0 ? -g : g;
-  return den;
-}
-
-// Per-block partial sums for Olsen's correction: a_j = sum_i x_i r_i / (theta_j - D_i),
-// b_j = sum_i x_i^2 / (theta_j - D_i) over this block's rows.
-__global__ void k_olsen_part(const double* __restrict__ X, const double* __restrict__ HX, int ldx,
-                             const double* __restrict__ diag, int64_t n,
-                             const int* __restrict__ cols, const double* __restrict__ theta,
-                             int nc, double* __restrict__ part) {
-  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t lo = blockIdx.x * per, hi = min(n, lo + per);
-  for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-    const int c = cols[j];
-    const double th = theta[c];
-    double a = 0.0, b = 0.0;
-    for (int64_t i = lo; i < hi; ++i) {
-      const double x = X[i * ldx + c];
-      const double r = HX[i * ldx + c] - th * x;
-      const double den = precond_den(th, diag[i]);
-      a += x * r / den;
-      b += x * x / den;
-    }
-    part[(int64_t)blockIdx.x * 2 * nc + j] = a;
-    part[(int64_t)blockIdx.x * 2 * nc + nc + j] = b;
-  }
-}
-
-__global__ void k_olsen_eps(const double* __restrict__ part, int nblk, int nc,
-                            double* __restrict__ eps) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nc; j += gridDim.x * blockDim.x) {
-    double a = 0.0, b = 0.0;
-    for (int q = 0; q < nblk; ++q) {
-      a += part[(int64_t)q * 2 * nc + j];
-      b += part[(int64_t)q * 2 * nc + nc + j];
-    }
-    eps[j] = (fabs(b) > 1e-300) ? a / b : 0.0;
-  }
-}
-
-// t_i = (r_i - eps_j x_i) / (theta_j - D_i): the diagonal-preconditioned residual made orthogonal
-// to the Ritz vector in the preconditioner's metric (Olsen's correction), which keeps Davidson
-// from stalling when the plain correction turns parallel to the Ritz vector.
-__global__ void k_correction(const double* __restrict__ X, const double* __restrict__ HX, int ldx,
-                             const double* __restrict__ diag, int64_t n,
-                             const int* __restrict__ cols, const double* __restrict__ theta,
-                             const double* __restrict__ eps, int nc, double* __restrict__ T,
-                             int ldt) {
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n * nc;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = idx / nc;
-    const int j = (int)(idx % nc);
-    const int c = cols[j];
-    const double th = theta[c];
-    const double x = X[i * ldx + c];
-    const double r = HX[i * ldx + c] - th * x;
-    T[i * ldt + j] = (r - eps[j] * x) / precond_den(th, diag[i]);
-  }
-}
-
 __global__ void k_copy_cols(const double* __restrict__ src, int lds, double* __restrict__ dst,
                             int ldd, int64_t n, int ncol) {
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n * ncol;
@@ -499,11 +436,6 @@ __global__ void k_fill_zero(double* p, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     p[i] = 0.0;
-}
-
-__global__ void k_set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nr) X[rows[r] * ldx + col0 + r] = 1.0;
 }
 
 }  // namespace
@@ -633,19 +565,6 @@ void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk
   note_launch(); k_sum_parts<<<(kk + 255) / 256, 256, 0, s>>>(part, nblk, kk, rn2, 0);
 }
 
-int correction_scratch(int64_t n, int nc) { return residual_blocks(n) * 2 * nc + nc; }
-
-void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
-                         int64_t n, const int* cols, const double* theta, int nc, double* T,
-                         int ldt, double* scratch, cudaStream_t s) {
-  if (nc <= 0 || n <= 0) return;
-  const int nblk = residual_blocks(n);
-  double* eps = scratch + (int64_t)nblk * 2 * nc;
-  note_launch(); k_olsen_part<<<nblk, 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, nc, scratch);
-  note_launch(); k_olsen_eps<<<(nc + 255) / 256, 256, 0, s>>>(scratch, nblk, nc, eps);
-  note_launch(); k_correction<<<grid_for(n * nc, 256), 256, 0, s>>>(X, HX, ldx, diag, n, cols, theta, eps, nc, T, ldt);
-}
-
 void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,
                cudaStream_t s) {
   if (n <= 0 || ncol <= 0) return;
@@ -661,10 +580,6 @@ void dense_from_csr(int64_t n, const int64_t* rowptr, const int32_t* col, const 
 
 void fill_zero(double* p, int64_t n, cudaStream_t s) {
   if (n > 0) { note_launch(); k_fill_zero<<<grid_for(n, 256), 256, 0, s>>>(p, n); }
-}
-
-void set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr, cudaStream_t s) {
-  if (nr > 0) { note_launch(); k_set_unit_rows<<<(nr + 127) / 128, 128, 0, s>>>(X, ldx, col0, rows, nr); }
 }
 
 void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cudaStream_t s) {

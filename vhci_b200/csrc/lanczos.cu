@@ -3,8 +3,9 @@
 // Ham.cpp:347-370), organised for the GPU:
 //   * blocks of b = 16 vectors; the SpMM gathers from a compact n x b copy of the block and
 //     streams the matrix from HBM once per block;
-//   * full reorthogonalisation (classical Gram-Schmidt, two passes) with FP64 GEMMs, and the
-//     projected matrix T = Q^T H Q formed explicitly from the stored H Q blocks;
+//   * full reorthogonalisation (classical Gram-Schmidt, two passes) with FP64 tensor-core
+//     projections (k_proj.cu), and the projected matrix T = Q^T H Q formed explicitly from the
+//     stored H Q blocks;
 //   * Rayleigh-Ritz (cuSOLVER syevd on T) only when the subspace is full; the kk = k + guard
 //     lowest Ritz vectors are kept (thick restart) together with the pending Lanczos block, so the
 //     kept Ritz vectors' residuals lie in the new subspace (Krylov-Schur property);
@@ -18,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -77,13 +79,51 @@ void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std::vecto
 }
 
 struct LWork {
-  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc;
+  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc, gpart;
   void release(cudaStream_t s) {
     Q.release(s); HQ.release(s); T.release(s); Yw.release(s); theta.release(s); Xb.release(s);
     HXb.release(s); W.release(s); S.release(s); M.release(s); part.release(s); rn2.release(s);
-    Xc.release(s);
+    Xc.release(s); gpart.release(s);
   }
 };
+
+// VHCI_PROJ=blas runs the projections through cuBLAS instead (comparison runs only).
+bool proj_blas() {
+  static const bool b = [] {
+    const char* e = std::getenv("VHCI_PROJ");
+    return e && std::string(e) == "blas";
+  }();
+  return b;
+}
+
+// Projections over the basis rows, on the FP64 tensor pipe (k_proj.cu).
+// C (M x P, column-major) = alpha A^T B + beta C, A n x M and B n x P row-major.
+int gemm_gram(vhci_ctx* c, LWork& w, const double* A, int lda, const double* B, int ldb, int64_t n,
+              int M, int P, double alpha, double beta, double* C, int ldc) {
+  if (M <= 0 || P <= 0) return VHCI_OK;
+  if (proj_blas()) {
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, M, P, (int)n, &alpha, A, lda, B, ldb, &beta,
+                    C, ldc));
+    return VHCI_OK;
+  }
+  VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
+  if (!proj_gram(A, lda, B, ldb, n, M, P, alpha, beta, C, ldc, w.gpart.p, c->st))
+    return fail(c, VHCI_E_INPUT, "projection with more than 16 right-hand columns");
+  return VHCI_OK;
+}
+
+// Out (n x P row-major) = alpha A S + beta Out, A n x M row-major, S M x P column-major.
+int gemm_rows(vhci_ctx* c, const double* A, int lda, const double* S, int lds, int64_t n, int M,
+              int P, double alpha, double beta, double* Out, int ldo) {
+  if (n <= 0 || P <= 0) return VHCI_OK;
+  if (proj_blas()) {
+    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, P, (int)n, M, &alpha, S, lds, A, lda, &beta,
+                    Out, ldo));
+    return VHCI_OK;
+  }
+  proj_rows(A, lda, S, lds, n, M, P, alpha, beta, Out, ldo, c->st);
+  return VHCI_OK;
+}
 
 int syevd_l(vhci_ctx* c, double* A, int m, int lda, double* w) {
   int lwork = 0;
@@ -106,10 +146,8 @@ int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb
                int ldo, int* r) {
   *r = 0;
   if (nb <= 0) return VHCI_OK;
-  const double one = 1.0, zero = 0.0;
   VCK(w.S.reserve((size_t)nb * nb, c->st));
-  VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, (int)n, &one, B, ld, B, ld, &zero,
-                  w.S.p, nb));
+  VTRY(gemm_gram(c, w, B, ld, B, ld, (int)n, nb, nb, 1.0, 0.0, w.S.p, nb));
   std::vector<double> S((size_t)nb * nb);
   VCK(d2h(c, S.data(), w.S.p, S.size() * sizeof(double)));
   VCK(cudaStreamSynchronize(c->st));
@@ -137,8 +175,7 @@ int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb
   }
   VCK(w.M.reserve(Mh.size(), c->st));
   VCK(h2d(c, w.M.p, Mh.data(), Mh.size() * sizeof(double)));
-  VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, rr, (int)n, nb, &one, w.M.p, nb, B, ld, &zero,
-                  out, ldo));
+  VTRY(gemm_rows(c, B, ld, w.M.p, nb, (int)n, nb, rr, 1.0, 0.0, out, ldo));
   *r = rr;
   return VHCI_OK;
 }
@@ -231,7 +268,6 @@ int block_lanczos(vhci_ctx* c, int k) {
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
-  const double one = 1.0, zero = 0.0, mone = -1.0;
   const double tol = c->o.eig_tol > 0 ? c->o.eig_tol : 1e-10;
   const double eps23 = std::pow(DBL_EPSILON, 2.0 / 3.0);
   const char* prof = std::getenv("VHCI_PROFILE");
@@ -270,8 +306,7 @@ int block_lanczos(vhci_ctx* c, int k) {
     DBuf<double> R;
     VCK(R.reserve(rnd.size(), s));
     VCK(h2d(c, R.p, rnd.data(), rnd.size() * sizeof(double)));
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, b, (int)c->x_rows, w0, &one, R.p, w0, c->X.p,
-                    c->ldx, &zero, w.W.p, b));
+    VTRY(gemm_rows(c, c->X.p, c->ldx, R.p, w0, (int)c->x_rows, w0, b, 1.0, 0.0, w.W.p, b));
     if (c->x_rows < n) fill_zero(w.W.p + (size_t)c->x_rows * b, (n - c->x_rows) * (int64_t)b, s);
     VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
     VCK(cudaStreamSynchronize(s));
@@ -309,8 +344,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       t0 = now();
       ++steps;
       // T[0:m+p, m:m+p] = Q^T (H Q_new)
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m + p, p, (int)n, &one, w.Q.p, ld,
-                      w.HQ.p + m, ld, &zero, w.T.p + (size_t)m * ld, ld));
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.HQ.p + m, ld, (int)n, m + p, p, 1.0, 0.0, w.T.p + (size_t)m * ld, ld));
       m += p;
       if (m + b > mmax || m >= n) {
         if (plevel) { cudaStreamSynchronize(s); t_orth += msince(t0); }
@@ -318,15 +352,13 @@ int block_lanczos(vhci_ctx* c, int k) {
       }
       // next block: W = H Q_new - Q T[:, new]; second Gram-Schmidt pass; SVQB
       copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, n, p, s);
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.T.p + (size_t)(m - p) * ld,
-                      ld, w.Q.p, ld, &one, w.W.p, b));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, (int)n, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)std::max(m, b) * p, s));
       bool second = true;
       if (kappa_max > 0) {
         // ||H q_c||^2 = ||T[:, c]||^2 + ||w_c||^2: the first pass removed the part of H q_c in
         // span(Q); a classical pass leaves an orthogonality error of about eps * ||H q_c|| / ||w_c||
-        VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, p, p, (int)n, &one, w.W.p, b, w.W.p, b,
-                        &zero, w.S.p, p));
+        VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, (int)n, p, p, 1.0, 0.0, w.S.p, p));
         std::vector<double> G((size_t)p * p), Tc((size_t)m * p);
         VCK(d2h(c, G.data(), w.S.p, G.size() * sizeof(double)));
         VCK(cudaMemcpy2DAsync(Tc.data(), m * sizeof(double), w.T.p + (size_t)(m - p) * ld,
@@ -343,10 +375,8 @@ int block_lanczos(vhci_ctx* c, int k) {
         if (!second) ++skipped;
       }
       if (second) {
-        VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, p, (int)n, &one, w.Q.p, ld, w.W.p, b,
-                        &zero, w.S.p, m));
-        VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.S.p, m, w.Q.p, ld,
-                        &one, w.W.p, b));
+        VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, (int)n, m, p, 1.0, 0.0, w.S.p, m));
+        VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, (int)n, m, p, -1.0, 1.0, w.W.p, b));
       }
       int p2 = 0;
       VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + m, ld, &p2));
@@ -361,10 +391,8 @@ int block_lanczos(vhci_ctx* c, int k) {
                           m * sizeof(double), m, cudaMemcpyDeviceToDevice, s));
     VTRY(syevd_l(c, w.Yw.p, m, ld, w.theta.p));
     const int nk = std::min(kk, m);
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nk, (int)n, m, &one, w.Yw.p, ld, w.Q.p, ld,
-                    &zero, w.Xb.p, kk));
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nk, (int)n, m, &one, w.Yw.p, ld, w.HQ.p, ld,
-                    &zero, w.HXb.p, kk));
+    VTRY(gemm_rows(c, w.Q.p, ld, w.Yw.p, ld, (int)n, m, nk, 1.0, 0.0, w.Xb.p, kk));
+    VTRY(gemm_rows(c, w.HQ.p, ld, w.Yw.p, ld, (int)n, m, nk, 1.0, 0.0, w.HXb.p, kk));
     residual_norms(w.Xb.p, w.HXb.p, n, kk, nk, w.theta.p, w.part.p, nblk, w.rn2.p, s);
     VCK(d2h(c, th.data(), w.theta.p, nk * sizeof(double)));
     VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
@@ -399,13 +427,10 @@ int block_lanczos(vhci_ctx* c, int k) {
     // ---- thick restart: pending block from the last expansion, then keep the Ritz block
     t0 = now();
     copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, n, p, s);
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.T.p + (size_t)(m - p) * ld,
-                    ld, w.Q.p, ld, &one, w.W.p, b));
+    VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, (int)n, m, p, -1.0, 1.0, w.W.p, b));
     VCK(w.S.reserve((size_t)m * p, s));
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, p, (int)n, &one, w.Q.p, ld, w.W.p, b,
-                    &zero, w.S.p, m));
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.S.p, m, w.Q.p, ld,
-                    &one, w.W.p, b));
+    VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, (int)n, m, p, 1.0, 0.0, w.S.p, m));
+    VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, (int)n, m, p, -1.0, 1.0, w.W.p, b));
     copy_cols(w.Xb.p, kk, w.Q.p, ld, n, nk, s);
     copy_cols(w.HXb.p, kk, w.HQ.p, ld, n, nk, s);
     int p2 = 0;
@@ -454,7 +479,6 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
   const int span = 2;
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   const int ld = (mmax + b + 15) / 16 * 16;
-  const double one = 1.0, zero = 0.0, mone = -1.0;
   const double tol = c->o.eig_tol > 0 ? c->o.eig_tol : 1e-10;
   const double eps23 = std::pow(DBL_EPSILON, 2.0 / 3.0);
   const char* prof = std::getenv("VHCI_PROFILE");
@@ -490,8 +514,7 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
     DBuf<double> R;
     VCK(R.reserve(rnd.size(), s));
     VCK(h2d(c, R.p, rnd.data(), rnd.size() * sizeof(double)));
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, b, (int)c->x_rows, w0, &one, R.p, w0, c->X.p,
-                    c->ldx, &zero, w.W.p, b));
+    VTRY(gemm_rows(c, c->X.p, c->ldx, R.p, w0, (int)c->x_rows, w0, b, 1.0, 0.0, w.W.p, b));
     if (c->x_rows < n) fill_zero(w.W.p + (size_t)c->x_rows * b, (n - c->x_rows) * (int64_t)b, s);
     VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
     VCK(cudaStreamSynchronize(s));
@@ -512,8 +535,7 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
   auto rotate = [&](int mm, int nk) -> int {
     for (int64_t r0 = 0; r0 < n; r0 += chunk) {
       const int64_t rows = std::min(chunk, n - r0);
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, nk, (int)rows, mm, &one, w.Yw.p, ld,
-                      w.Q.p + (size_t)r0 * ld, ld, &zero, w.Xb.p, nk));
+      VTRY(gemm_rows(c, w.Q.p + (size_t)r0 * ld, ld, w.Yw.p, ld, (int)rows, mm, nk, 1.0, 0.0, w.Xb.p, nk));
       VCK(cudaMemcpy2DAsync(w.Q.p + (size_t)r0 * ld, ld * sizeof(double), w.Xb.p,
                             nk * sizeof(double), nk * sizeof(double), rows,
                             cudaMemcpyDeviceToDevice, s));
@@ -531,19 +553,15 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
     while (true) {
       VTRY(apply_h_l(c, w, w.Q.p + m, ld, p, w.HQ.p, b));
       ++steps;
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m + p, p, (int)n, &one, w.Q.p, ld,
-                      w.HQ.p, b, &zero, w.T.p + (size_t)m * ld, ld));
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.HQ.p, b, (int)n, m + p, p, 1.0, 0.0, w.T.p + (size_t)m * ld, ld));
       m += p;
       plast = p;
       // pending block W = H Q_new - Q T[:, new], second Gram-Schmidt pass
       VCK(cudaMemcpyAsync(w.W.p, w.HQ.p, (size_t)n * b * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.T.p + (size_t)(m - p) * ld,
-                      ld, w.Q.p, ld, &one, w.W.p, b));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, (int)n, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)m * p, s));
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, p, (int)n, &one, w.Q.p, ld, w.W.p, b,
-                      &zero, w.S.p, m));
-      VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, p, (int)n, m, &mone, w.S.p, m, w.Q.p, ld,
-                      &one, w.W.p, b));
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, (int)n, m, p, 1.0, 0.0, w.S.p, m));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, (int)n, m, p, -1.0, 1.0, w.W.p, b));
       if (m + b > mmax || m >= n) break;
       int p2 = 0;
       VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + m, ld, &p2));
@@ -560,8 +578,7 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
     VCK(d2h(c, th.data(), w.theta.p, m * sizeof(double)));
     // residual estimates from the pending block: G = W^T W (plast x plast), Y's last-block rows
     VCK(w.S.reserve((size_t)plast * plast, s));
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, plast, plast, (int)n, &one, w.W.p, b, w.W.p,
-                    b, &zero, w.S.p, plast));
+    VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, (int)n, plast, plast, 1.0, 0.0, w.S.p, plast));
     G.resize((size_t)plast * plast);
     Yl.resize((size_t)plast * nk);
     VCK(d2h(c, G.data(), w.S.p, G.size() * sizeof(double)));

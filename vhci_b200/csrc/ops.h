@@ -127,23 +127,28 @@ void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, con
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
           const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
           int ldy, cudaStream_t s);
-// ---- Davidson helpers ----
+// ---- eigensolver helpers ----
 // rn2[c] (c < kk) = sum_i (HX[i,c] - theta[c] X[i,c])^2   (block partials reduced on device)
 void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,
                     const double* theta, double* part, int nblk, double* rn2, cudaStream_t s);
 int residual_blocks(int64_t n);
-// Olsen-corrected diagonal-preconditioned residuals of the Ritz pairs c_j = cols[j]:
-// T[i, j] = (r_i - eps_j x_i) / (theta_j - d_i).  scratch holds correction_scratch(n, nc) doubles.
-int correction_scratch(int64_t n, int nc);
-void davidson_correction(const double* X, const double* HX, int ldx, const double* diag,
-                         int64_t n, const int* cols, const double* theta, int nc, double* T,
-                         int ldt, double* scratch, cudaStream_t s);
 void copy_cols(const double* src, int lds, double* dst, int ldd, int64_t n, int ncol,
                cudaStream_t s);
 void dense_from_csr(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
                     const float* valf, const double* diag, double* A, cudaStream_t s);
 void fill_zero(double* p, int64_t n, cudaStream_t s);
-void set_unit_rows(double* X, int ldx, int col0, const int64_t* rows, int nr, cudaStream_t s);
+
+// ---- FP64 tensor-core projections (k_proj.cu) ----
+// C (M x P, column-major, ldc) = alpha A^T B + beta C with A n x M and B n x P row-major (lda,
+// ldb); any M (slabs of 1024), P <= 16; part holds proj_gram_scratch(M, P) doubles.  Returns
+// false (nothing launched) for P > 16 or strides shorter than the rows.
+int64_t proj_gram_scratch(int M, int P);
+bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, int M, int P,
+               double alpha, double beta, double* C, int ldc, double* part, cudaStream_t s);
+// Out (n x P row-major, ldo) = alpha A S + beta Out with A n x M row-major and S M x P
+// column-major (lds); any P (column chunks of 64).
+void proj_rows(const double* A, int lda, const double* S, int lds, int64_t n, int M, int P,
+               double alpha, double beta, double* Out, int ldo, cudaStream_t s);
 
 // ---- PT2 (k_pt2.cu) ----
 void pt2_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
