@@ -217,6 +217,37 @@ vhci_status vhci_read_checkpoint(vhci_ctx* c, const char* path);
 /* Eigenvalues currently held (n <= k). */
 vhci_status vhci_get_energies(const vhci_ctx* c, double* E, int k, int* n);
 
+/* ---- one solve sharded over several GPUs ---------------------------------------------------
+ * No counterpart in the reference program, which runs in one address space (its loops are OpenMP
+ * threads over one basis, Ham.cpp:237, PT2.cpp:66).  With a communicator set, the ranks (one
+ * context per GPU, each built from the same input) solve one problem together:
+ *  - the Hamiltonian's rows and the eigensolver's Krylov basis are split into contiguous row
+ *    blocks of ceil(n / nranks) rows, one per rank;
+ *  - before every sparse product the ranks' blocks of the vector block are all-gathered, and the
+ *    projections' partial sums (Gram matrices, residual norms) are all-reduced; the projected
+ *    eigenproblem is solved on rank 0 and broadcast;
+ *  - after each eigensolve the Ritz vectors are all-gathered, so heat-bath selection runs on every
+ *    rank with identical results;
+ *  - PT2 splits the perturber space into one contiguous range per rank and all-reduces the
+ *    corrections.
+ * The collectives are the caller's (for example torch.distributed over NCCL).  The library
+ * synchronises its stream before each call; a callback must finish the collective (the buffers
+ * are device memory of the context's device) before it returns 0.  Every rank must make the same
+ * sequence of library calls.  Bases whose eigensolve is dense (up to 2000 states, and the first
+ * heat-bath step) are solved whole on every rank.  vhci_apply_h, vhci_residual_norms(_noalloc)
+ * and vhci_get_h_csr return VHCI_E_STATE on a sharded context. */
+typedef struct {
+  int rank, nranks;
+  void* user;
+  /* sum `count` doubles of buf over the ranks, in place */
+  int (*allreduce_sum)(void* user, double* buf, int64_t count);
+  /* recv (nranks * bytes bytes) = the ranks' `bytes`-byte send buffers in rank order */
+  int (*allgather)(void* user, const void* send, void* recv, int64_t bytes);
+} vhci_comm;
+
+/* Set (or, with NULL or nranks == 1, clear) the communicator; call before vhci_hci. */
+vhci_status vhci_set_comm(vhci_ctx* c, const vhci_comm* comm);
+
 /* ---- request server (continuous batching of independent solves on one GPU) ----------------
  * No counterpart in the reference program, which solves one input per process.  Each request is
  * a reference-format input file (or an in-memory problem) with an arrival time in seconds after

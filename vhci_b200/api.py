@@ -30,6 +30,7 @@ EXPORTS = [
     "vhci_structural_nnz", "vhci_eigs", "vhci_hci", "vhci_pt2", "vhci_write_freqs",
     "vhci_write_checkpoint", "vhci_read_checkpoint", "vhci_get_energies", "vhci_apply_h",
     "vhci_residual_norms", "vhci_residual_norms_noalloc", "vhci_default_serve_opts", "vhci_serve",
+    "vhci_set_comm",
 ]
 
 
@@ -67,6 +68,18 @@ class Info(ctypes.Structure):
 
 # void (*vhci_iter_cb)(void* user, int iteration, int64_t n_basis, double zpe)
 ITER_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double)
+
+
+# int (*allreduce_sum)(void* user, double* buf, int64_t count)
+ALLREDUCE_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)
+# int (*allgather)(void* user, const void* send, void* recv, int64_t bytes)
+ALLGATHER_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_int64)
+
+
+class Comm(ctypes.Structure):
+    _fields_ = [("rank", ctypes.c_int), ("nranks", ctypes.c_int), ("user", ctypes.c_void_p),
+                ("allreduce_sum", ALLREDUCE_CB), ("allgather", ALLGATHER_CB)]
 
 
 class Request(ctypes.Structure):
@@ -159,6 +172,7 @@ def lib():
             "vhci_write_checkpoint": (ctypes.c_int, [vp, ctypes.c_char_p]),
             "vhci_read_checkpoint": (ctypes.c_int, [vp, ctypes.c_char_p]),
             "vhci_get_energies": (ctypes.c_int, [vp, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+            "vhci_set_comm": (ctypes.c_int, [vp, ctypes.POINTER(Comm)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -356,6 +370,13 @@ class VHCI:
         self._check(lib().vhci_residual_norms_noalloc(self.h, ctypes.c_void_p(x_dev),
                                                       ctypes.c_void_p(theta_dev),
                                                       ctypes.c_void_p(rnorm_dev), k))
+
+    def set_comm(self, comm) -> None:
+        """Shard this context's solve over the ranks of `comm` (a vhci_b200.shard.Comm, or None to
+        solve alone).  Every rank must create its context from the same input and make the same
+        calls."""
+        self._comm = comm  # the callbacks must outlive the context's use of them
+        self._check(lib().vhci_set_comm(self.h, ctypes.byref(comm.struct) if comm else None))
 
     def eigs(self, k: int) -> np.ndarray:
         E = np.zeros(k)

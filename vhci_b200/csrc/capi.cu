@@ -404,11 +404,11 @@ double device_available(vhci_ctx* c) {
 void spmm_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
   const bool f = c->o.precision == 1;
   if (c->npanel > 0)
-    spmm_panels(c->n, c->npanel, c->prow.p, c->pcol.p, f ? nullptr : c->pval.p,
-                f ? c->pvalf.p : nullptr, c->diag.p, X, ldx, b, Y, ldy, c->st);
+    spmm_panels(c->nrow, c->npanel, c->prow.p, c->pcol.p, f ? nullptr : c->pval.p,
+                f ? c->pvalf.p : nullptr, c->diag.p, X, ldx, b, Y, ldy, c->row0, c->st);
   else
-    spmm(c->n, c->rowptr.p, c->col.p, f ? nullptr : c->val.p, f ? c->valf.p : nullptr,
-         c->diag.p, X, ldx, b, Y, ldy, c->st);
+    spmm(c->nrow, c->rowptr.p, c->col.p, f ? nullptr : c->val.p, f ? c->valf.p : nullptr,
+         c->diag.p, X, ldx, b, Y, ldy, c->row0, c->st);
 }
 
 // Column panels for the product: one 16-column FP64 block row is 128 bytes, and each panel's rows
@@ -419,7 +419,8 @@ void spmm_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
 // in free device memory.
 static int build_panels(vhci_ctx* c) {
   c->npanel = 0;
-  const int64_t n = c->n;
+  const int64_t n = c->n;      // columns
+  const int64_t nr = c->nrow;  // rows held
   if (const char* e = std::getenv("VHCI_PANELS"))
     if (std::atoi(e) == 0) return VHCI_OK;
   double pbytes = 96e6;
@@ -429,7 +430,7 @@ static int build_panels(vhci_ctx* c) {
   P = std::min(P, kMaxPanels);
   const int64_t cw = (n + P - 1) / P;
   P = (int)((n + cw - 1) / cw);
-  const int64_t pn = (int64_t)P * n;
+  const int64_t pn = (int64_t)P * nr;
   const double sval = c->o.precision == 1 ? 4.0 : 8.0;
   const double need = (double)c->nnz * (4.0 + sval) + (pn + 1) * 8.0 + pn * 4.0 +
                       scan_tmp_elems(pn) * 8.0 + 2e9;
@@ -440,14 +441,14 @@ static int build_panels(vhci_ctx* c) {
   DBuf<int64_t> tmp;
   VCK(cnt.reserve(pn, c->st));
   VCK(cudaMemsetAsync(cnt.p, 0, pn * sizeof(int32_t), c->st));
-  panel_count(n, c->rowptr.p, c->col.p, cw, cnt.p, c->st);
+  panel_count(nr, c->rowptr.p, c->col.p, cw, cnt.p, c->st);
   VCK(c->prow.reserve(pn + 1, c->st));
   VCK(tmp.reserve(std::max<int64_t>(scan_tmp_elems(pn), 1), c->st));
   exclusive_scan_i32(cnt.p, c->prow.p, pn, tmp.p, c->st);
   VCK(c->pcol.reserve(c->nnz, c->st));
   if (c->o.precision == 1) VCK(c->pvalf.reserve(c->nnz, c->st));
   else VCK(c->pval.reserve(c->nnz, c->st));
-  panel_fill(n, c->rowptr.p, c->col.p, c->o.precision == 1 ? nullptr : c->val.p,
+  panel_fill(nr, c->rowptr.p, c->col.p, c->o.precision == 1 ? nullptr : c->val.p,
              c->o.precision == 1 ? c->valf.p : nullptr, cw, P, c->prow.p, c->pcol.p, c->pval.p,
              c->pvalf.p, c->st);
   cnt.release(c->st);
@@ -493,7 +494,7 @@ int structural_count(vhci_ctx* c, int64_t* out) {
   VCK(c->rowcnt.reserve(n, c->st));
   VCK(sum.reserve(n + 1, c->st));
   VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(n), 1), c->st));
-  hbuild_count(c->keys.p, n, c->L, basis_view(c), d, c->rowcnt.p, c->st);
+  hbuild_count(c->keys.p, 0, n, c->L, basis_view(c), d, c->rowcnt.p, c->st);
   exclusive_scan_i32(c->rowcnt.p, sum.p, n, c->scan_tmp.p, c->st);
   int64_t pairs = 0;
   VCK(d2h(c, &pairs, sum.p + n, sizeof(int64_t)));
@@ -503,21 +504,70 @@ int structural_count(vhci_ctx* c, int64_t* out) {
   return VHCI_OK;
 }
 
-int build_h(vhci_ctx* c) {
+// ---- collectives of a sharded solve ---------------------------------------------------------
+// The callbacks run the caller's collectives on device buffers; the stream is synchronised first
+// so the buffers hold their final values, and the callback completes the collective before it
+// returns.
+
+int comm_sum(vhci_ctx* c, double* buf, int64_t count) {
+  if (!is_sharded(c) || count <= 0) return VHCI_OK;
+  VCK(cudaStreamSynchronize(c->st));
+  if (c->comm.allreduce_sum(c->comm.user, buf, count) != 0)
+    return fail(c, VHCI_E_CUDA, "all-reduce of the sharded solve failed");
+  return VHCI_OK;
+}
+
+int comm_gather(vhci_ctx* c, const void* send, void* recv, int64_t bytes) {
+  if (!is_sharded(c)) {
+    if (recv != send && bytes > 0)
+      VCK(cudaMemcpyAsync(recv, send, bytes, cudaMemcpyDeviceToDevice, c->st));
+    return VHCI_OK;
+  }
+  VCK(cudaStreamSynchronize(c->st));
+  if (c->comm.allgather(c->comm.user, send, recv, bytes) != 0)
+    return fail(c, VHCI_E_CUDA, "all-gather of the sharded solve failed");
+  return VHCI_OK;
+}
+
+int comm_bcast0(vhci_ctx* c, double* buf, int64_t count) {
+  if (!is_sharded(c) || count <= 0) return VHCI_OK;
+  if (c->comm.rank != 0) VCK(cudaMemsetAsync(buf, 0, count * sizeof(double), c->st));
+  return comm_sum(c, buf, count);
+}
+
+bool dense_path(int64_t n, int k) {
+  const int guard = std::max(4, k / 10);
+  const int64_t kk = std::min<int64_t>(n, k + guard);
+  return n <= 2000 || n <= 3 * kk + 64;
+}
+
+int build_h(vhci_ctx* c, bool all_rows) {
   const int64_t n = c->n;
   c->npanel = 0;
   c->pcol.release(c->st);  // the previous panels: freed before the new matrix is built
   c->pval.release(c->st);
   c->pvalf.release(c->st);
   c->prow.release(c->st);
+  // rows held: every row, or this rank's block when the solve is sharded and sparse
+  c->h_rows = !all_rows && is_sharded(c) && !dense_path(n, c->M.nstate);
+  if (c->h_rows) {
+    c->rblk = (n + c->comm.nranks - 1) / c->comm.nranks;
+    c->row0 = std::min<int64_t>(n, (int64_t)c->comm.rank * c->rblk);
+    c->nrow = std::min<int64_t>(c->rblk, n - c->row0);
+  } else {
+    c->row0 = 0;
+    c->nrow = n;
+    c->rblk = n;
+  }
+  const int64_t r0 = c->row0, nr = c->nrow;
   VCK(cudaEventRecord(c->ev_a, c->st));
-  VCK(c->rowcnt.reserve(n, c->st));
-  VCK(c->rowptr.reserve(n + 1, c->st));
-  VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(n), 1), c->st));
-  hbuild_count(c->keys.p, n, c->L, basis_view(c), conn_view(c), c->rowcnt.p, c->st);
-  exclusive_scan_i32(c->rowcnt.p, c->rowptr.p, n, c->scan_tmp.p, c->st);
+  VCK(c->rowcnt.reserve(std::max<int64_t>(nr, 1), c->st));
+  VCK(c->rowptr.reserve(nr + 1, c->st));
+  VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(nr), 1), c->st));
+  hbuild_count(c->keys.p, r0, nr, c->L, basis_view(c), conn_view(c), c->rowcnt.p, c->st);
+  exclusive_scan_i32(c->rowcnt.p, c->rowptr.p, nr, c->scan_tmp.p, c->st);
   int64_t nnz = 0;
-  VCK(d2h(c, &nnz, c->rowptr.p + n, sizeof(int64_t)));
+  VCK(d2h(c, &nnz, c->rowptr.p + nr, sizeof(int64_t)));
   VCK(cudaStreamSynchronize(c->st));
   // the previous matrix's arrays are replaced, not grown in place: release them first so the old
   // and new matrix never coexist
@@ -525,15 +575,15 @@ int build_h(vhci_ctx* c) {
   if ((int64_t)c->val.cap < nnz) c->val.release(c->st);
   if ((int64_t)c->valf.cap < nnz) c->valf.release(c->st);
   {  // admission: the matrix and the eigensolver's smallest working set must fit together
-    const double hbytes = (double)nnz * (4.0 + (c->o.precision == 1 ? 4.0 : 8.0)) + 8.0 * n;
+    const double hbytes = (double)nnz * (4.0 + (c->o.precision == 1 ? 4.0 : 8.0)) + 8.0 * nr;
     const double avail = device_available(c) + 8.0 * (double)c->x_rows * c->ldx;
     const double eig = lanczos_min_bytes(c, c->M.nstate);
     if (hbytes + eig > avail) {
       char msg[320];
       std::snprintf(msg, sizeof msg,
-                    "Hamiltonian of %lld states and %lld off-diagonal entries needs %.1f GB (plus "
-                    "%.1f GB for the eigensolver); %.1f GB of device memory is available",
-                    (long long)n, (long long)nnz, hbytes / 1e9, eig / 1e9, avail / 1e9);
+                    "Hamiltonian rows of %lld states and %lld off-diagonal entries need %.1f GB "
+                    "(plus %.1f GB for the eigensolver); %.1f GB of device memory is available",
+                    (long long)nr, (long long)nnz, hbytes / 1e9, eig / 1e9, avail / 1e9);
       return fail(c, VHCI_E_OOM, msg);
     }
   }
@@ -543,8 +593,8 @@ int build_h(vhci_ctx* c) {
   } else {
     VCK(c->val.reserve(std::max<int64_t>(nnz, 1), c->st));
   }
-  VCK(c->diag.reserve(n, c->st));
-  hbuild_fill(c->keys.p, n, c->L, basis_view(c), conn_view(c), c->rowptr.p, c->col.p,
+  VCK(c->diag.reserve(std::max<int64_t>(nr, 1), c->st));
+  hbuild_fill(c->keys.p, r0, nr, c->L, basis_view(c), conn_view(c), c->rowptr.p, c->col.p,
               c->o.precision == 1 ? nullptr : c->val.p, c->o.precision == 1 ? c->valf.p : nullptr,
               c->diag.p, c->st);
   c->nnz = nnz;
@@ -553,7 +603,7 @@ int build_h(vhci_ctx* c) {
   VCK(cudaEventSynchronize(c->ev_b));
   VCK(cudaGetLastError());
   c->stats.ms_hbuild += event_ms(c);
-  c->stats.hbuild_probes += 2 * n * (int64_t)c->conn.groups.size();
+  c->stats.hbuild_probes += 2 * nr * (int64_t)c->conn.groups.size();
   c->nnz = nnz;
   c->h_valid = true;
   return VHCI_OK;
@@ -868,10 +918,24 @@ vhci_status vhci_build_h(vhci_ctx* c, int64_t* nnz) {
   return VHCI_OK;
 }
 
+vhci_status vhci_set_comm(vhci_ctx* c, const vhci_comm* comm) {
+  if (!c) return VHCI_E_INPUT;
+  if (!comm || comm->nranks <= 1) {
+    c->comm = vhci_comm{};
+  } else {
+    if (comm->rank < 0 || comm->rank >= comm->nranks || !comm->allreduce_sum || !comm->allgather)
+      return fail(c, VHCI_E_INPUT, "vhci_set_comm: bad rank or missing collective");
+    c->comm = *comm;
+  }
+  c->h_valid = false;  // the held matrix's rows follow the sharding
+  return VHCI_OK;
+}
+
 vhci_status vhci_get_h_csr(const vhci_ctx* c0, int64_t* rowptr, int32_t* col, double* val) {
   vhci_ctx* c = const_cast<vhci_ctx*>(c0);
   if (!c || !rowptr || !col || !val) return VHCI_E_INPUT;
   if (!c->h_valid) return fail(c, VHCI_E_STATE, "Hamiltonian not built");
+  if (c->h_rows) return fail(c, VHCI_E_STATE, "the Hamiltonian is sharded over the ranks");
   const int64_t n = c->n;
   std::vector<int64_t> rp(n + 1);
   std::vector<int32_t> cl(c->nnz);

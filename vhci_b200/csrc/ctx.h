@@ -102,6 +102,13 @@ struct vhci_ctx {
   vhci::DBuf<double> hbabs;
   vhci::DBuf<int64_t> hbcumd;
 
+  // sharded solve (vhci_set_comm, comm.nranks > 1): when h_rows is set the held Hamiltonian is
+  // the row block [row0, row0 + nrow) of the basis; every rank's block has rblk = ceil(n/nranks)
+  // rows (the last may be shorter), the layout of the gathered vector blocks
+  vhci_comm comm{};
+  bool h_rows = false;
+  int64_t row0 = 0, nrow = 0, rblk = 0;
+
   // Hamiltonian (off-diagonal CSR + FP64 diagonal)
   bool h_valid = false;
   int64_t nnz = 0;

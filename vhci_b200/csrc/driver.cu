@@ -50,19 +50,23 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     hash_clear(pslots.p, ns, s);
     hash_insert_range(pslots.p, ns - 1, pkeys.p, 0, np, L.W, c->flags.p, s);
     HashView pv{pslots.p, ns - 1, pkeys.p};
-    // entry counts per perturber row
+    // this rank's perturbers [A0, A1): all of them, or one contiguous share on a sharded context
+    // (the vectors are held whole on every rank, so each share is computed independently)
+    const int R = is_sharded(c) ? c->comm.nranks : 1, rk = is_sharded(c) ? c->comm.rank : 0;
+    const int64_t A0 = np * rk / R, A1 = np * (rk + 1) / R, NA = A1 - A0;
+    // entry counts per perturber row (row a at index a - A0)
     DBuf<int32_t> acount;
     DBuf<int64_t> arow, tmp;
-    VCK(acount.reserve(np, s));
-    VCK(arow.reserve(np + 1, s));
-    VCK(tmp.reserve(std::max<int64_t>(scan_tmp_elems(np), 1), s));
-    VCK(cudaMemsetAsync(acount.p, 0, np * sizeof(int32_t), s));
-    pt2_count(c->keys.p, n, L, pv, conn_view(c), 0, np, acount.p, s);
-    exclusive_scan_i32(acount.p, arow.p, np, tmp.p, s);
-    std::vector<int64_t> arow_h(np + 1);
-    VCK(d2h(c, arow_h.data(), arow.p, (np + 1) * sizeof(int64_t)));
+    VCK(acount.reserve(std::max<int64_t>(NA, 1), s));
+    VCK(arow.reserve(NA + 1, s));
+    VCK(tmp.reserve(std::max<int64_t>(scan_tmp_elems(NA), 1), s));
+    VCK(cudaMemsetAsync(acount.p, 0, std::max<int64_t>(NA, 1) * sizeof(int32_t), s));
+    pt2_count(c->keys.p, n, L, pv, conn_view(c), A0, A1, acount.p, s);
+    exclusive_scan_i32(acount.p, arow.p, NA, tmp.p, s);
+    std::vector<int64_t> arow_h(NA + 1);
+    VCK(d2h(c, arow_h.data(), arow.p, (NA + 1) * sizeof(int64_t)));
     VCK(cudaStreamSynchronize(s));
-    const int64_t total = arow_h[np];
+    const int64_t total = arow_h[NA];
     c->stats.pt2_entries += total;
     // chunk the perturber range so one chunk's entries fit the budget
     size_t freeb = 0, totb = 0;
@@ -70,20 +74,22 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     // entries (12 bytes) plus, in the worst case, the same again as scratch for long-row ordering
     int64_t budget = c->o.pt2_chunk > 0 ? c->o.pt2_chunk : (int64_t)(freeb * 0.4 / 12.0);
     budget = std::max<int64_t>(budget, 1 << 20);
-    std::vector<int64_t> bounds{0};
-    while (bounds.back() < np) {
+    // chunk bounds in perturber indices; arow_h is indexed from A0
+    std::vector<int64_t> bounds{A0};
+    while (bounds.back() < A1) {
       const int64_t a0 = bounds.back();
-      const int64_t lim = arow_h[a0] + budget;
-      int64_t a1 = std::upper_bound(arow_h.begin() + a0 + 1, arow_h.end(), lim) - arow_h.begin() - 1;
+      const int64_t lim = arow_h[a0 - A0] + budget;
+      int64_t a1 = A0 + (std::upper_bound(arow_h.begin() + (a0 - A0) + 1, arow_h.end(), lim) -
+                         arow_h.begin()) - 1;
       if (a1 <= a0) a1 = a0 + 1;
-      bounds.push_back(std::min(a1, np));
+      bounds.push_back(std::min(a1, A1));
     }
     DBuf<int32_t> ecol;
     DBuf<double> eval, part, dEd, Ed;
     const int64_t maxchunk = [&] {
       int64_t mx = 0;
       for (size_t q = 1; q < bounds.size(); ++q)
-        mx = std::max(mx, arow_h[bounds[q]] - arow_h[bounds[q - 1]]);
+        mx = std::max(mx, arow_h[bounds[q] - A0] - arow_h[bounds[q - 1] - A0]);
       return mx;
     }();
     VCK(ecol.reserve(std::max<int64_t>(maxchunk, 1), s));
@@ -102,7 +108,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       const int64_t a0 = bounds[q - 1], a1 = bounds[q];
       VCK(crow.reserve(a1 - a0 + 1, s));
       std::vector<int64_t> cr(a1 - a0 + 1);
-      for (int64_t a = a0; a <= a1; ++a) cr[a - a0] = arow_h[a] - arow_h[a0];
+      for (int64_t a = a0; a <= a1; ++a) cr[a - a0] = arow_h[a - A0] - arow_h[a0 - A0];
       VCK(h2d(c, crow.p, cr.data(), cr.size() * sizeof(int64_t)));
       VCK(cudaMemsetAsync(acount.p, 0, (a1 - a0) * sizeof(int32_t), s));
       pt2_fill(c->keys.p, n, L, pv, conn_view(c), a0, a1, crow.p, acount.p, ecol.p, eval.p, s);
@@ -143,6 +149,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       const int64_t ent = cr.back();
       c->stats.pt2_reduce_bytes += ent * (4 + 8) + ent * (int64_t)nopt * 8 + (a1 - a0) * (8 + 8 * L.W);
     }
+    VTRY(comm_sum(c, dEd.p, nopt));  // the ranks' shares of the perturber sum
     VCK(d2h(c, dE.data(), dEd.p, nopt * sizeof(double)));
     VCK(cudaStreamSynchronize(s));
     VCK(cudaGetLastError());

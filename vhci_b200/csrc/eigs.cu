@@ -66,7 +66,7 @@ int apply_h(vhci_ctx* c, const double* X, int ldx, int b, double* Y, int ldy) {
 
 int dense_eigs(vhci_ctx* c, int keep) {
   const int64_t n = c->n;
-  if (!c->h_valid) VTRY(build_h(c));
+  if (!c->h_valid || c->h_rows) VTRY(build_h(c, true));  // the dense solve needs every row
   keep = (int)std::min<int64_t>(keep, n);
   DBuf<double> A, w;
   VCK(A.reserve((size_t)n * n, c->st));
@@ -99,7 +99,7 @@ int eigs(vhci_ctx* c, int k) {
   const int guard = std::max(4, k / 10);
   const int kk = (int)std::min<int64_t>(n, k + guard);
   VCK(cudaEventRecord(c->ev_a, c->st));
-  const int r = (n <= 2000 || n <= 3 * (int64_t)kk + 64) ? dense_eigs(c, kk) : block_lanczos(c, k);
+  const int r = dense_path(n, k) ? dense_eigs(c, kk) : block_lanczos(c, k);
   if (r != VHCI_OK) return r;
   VCK(cudaEventRecord(c->ev_b, c->st));
   VCK(cudaEventSynchronize(c->ev_b));
@@ -113,7 +113,8 @@ using namespace vhci;
 
 extern "C" vhci_status vhci_apply_h(vhci_ctx* c, const double* X, double* Y, int b) {
   if (!c || !X || !Y || b <= 0) return VHCI_E_INPUT;
-  if (!c->h_valid) VTRY(build_h(c));
+  if (is_sharded(c)) return fail(c, VHCI_E_STATE, "vhci_apply_h on a sharded context");
+  if (!c->h_valid || c->h_rows) VTRY(build_h(c, true));
   const int64_t n = c->n;
   std::vector<double> h((size_t)n * b);
   for (int64_t i = 0; i < n; ++i)

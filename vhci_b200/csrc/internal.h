@@ -42,7 +42,20 @@ int append_keys(vhci_ctx* c, const uint64_t* dkeys, int64_t m);
 // count in c->nsel.  Promotes the key layout and retries when a state needs 8-bit fields.
 int generate_new_set(vhci_ctx* c, double eps);
 
-int build_h(vhci_ctx* c);
+// Builds the Hamiltonian: all rows, or this rank's row block when the context is sharded and the
+// eigensolve will be the sparse one (all_rows forces every row, as the dense solve needs).
+int build_h(vhci_ctx* c, bool all_rows = false);
+// The eigensolve of k pairs over n states is dense (small bases): every rank solves it whole.
+bool dense_path(int64_t n, int k);
+
+// ---- collectives of a sharded solve (no-ops on an unsharded context) ----
+inline bool is_sharded(const vhci_ctx* c) { return c->comm.nranks > 1; }
+// buf (device, count doubles) = its sum over the ranks
+int comm_sum(vhci_ctx* c, double* buf, int64_t count);
+// recv (device) = the ranks' `bytes`-byte send buffers in rank order
+int comm_gather(vhci_ctx* c, const void* send, void* recv, int64_t bytes);
+// buf = rank 0's values on every rank
+int comm_bcast0(vhci_ctx* c, double* buf, int64_t count);
 // Two CUDA events that are destroyed with their scope, so early error returns release them.
 struct EventPair {
   cudaEvent_t a = nullptr, b = nullptr;

@@ -23,10 +23,12 @@ inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
 namespace {
 
 // One warp per row; lanes stride over the connection groups, probe the basis hash and compact
-// the hits with a ballot, so a row's entries land in group order (deterministic layout).
+// the hits with a ballot, so a row's entries land in group order (deterministic layout).  Rows
+// row0 .. row0 + n - 1 of the basis are built (all of them, or one rank's block of a sharded
+// matrix); rowcnt, rowptr and diag are indexed from row0, columns are basis indices.
 template <int W, bool FILL>
-__global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ keys, int64_t n,
-                                                KeyLayout L, HashView basis, ConnDev cd,
+__global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ keys, int64_t row0,
+                                                int64_t n, KeyLayout L, HashView basis, ConnDev cd,
                                                 int32_t* __restrict__ rowcnt,
                                                 const int64_t* __restrict__ rowptr,
                                                 int32_t* __restrict__ col,
@@ -42,7 +44,7 @@ __global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ key
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
        i += warps) {
     uint64_t k[W];
-    load_key<W>(keys, i, k);
+    load_key<W>(keys, row0 + i, k);
     const int64_t pos = FILL ? rowptr[i] : 0;
     int cnt = 0;
     for_each_group<W>(cd, k, L, s_exc[threadIdx.x >> 5], s_binom, [&](int64_t u) {
@@ -70,116 +72,35 @@ __global__ void __launch_bounds__(256) k_hbuild(const uint64_t* __restrict__ key
 }
 
 template <int W>
-void hbuild_count_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
-                         int32_t* rowcnt, cudaStream_t s) {
+void hbuild_count_launch(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L,
+                         HashView basis, ConnDev cd, int32_t* rowcnt, cudaStream_t s) {
   note_launch(); k_hbuild<W, false><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
-      keys, n, L, basis, cd, rowcnt, nullptr, nullptr, nullptr, nullptr, nullptr);
+      keys, row0, n, L, basis, cd, rowcnt, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 template <int W>
-void hbuild_fill_launch(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
-                        const int64_t* rowptr, int32_t* col, double* val, float* valf,
-                        double* diag, cudaStream_t s) {
+void hbuild_fill_launch(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L,
+                        HashView basis, ConnDev cd, const int64_t* rowptr, int32_t* col,
+                        double* val, float* valf, double* diag, cudaStream_t s) {
   note_launch(); k_hbuild<W, true><<<grid_for(n * 32, 256, 148 * 8), 256, 0, s>>>(
-      keys, n, L, basis, cd, nullptr, rowptr, col, val, valf, diag);
+      keys, row0, n, L, basis, cd, nullptr, rowptr, col, val, valf, diag);
 }
 
-// Y = (D + H_off) X for b columns.  One warp per row; lanes own columns lane + 32 r; every
-// entry's X row is a contiguous b*8-byte gather (the rows are 16-byte aligned).
-template <int NR, typename VT>
-__global__ void __launch_bounds__(256) k_spmm(int64_t n, const int64_t* __restrict__ rowptr,
-                                              const int32_t* __restrict__ col,
-                                              const VT* __restrict__ val,
-                                              const double* __restrict__ diag,
-                                              const double* __restrict__ X, int ldx, int b,
-                                              double* __restrict__ Y, int ldy) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
-       i += warps) {
-    double acc[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-    const int64_t beg = rowptr[i], end = rowptr[i + 1];
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {
-      const int64_t e = e0 + lane;
-      int jj = 0;
-      double vv = 0.0;
-      if (e < end) { jj = __ldg(col + e); vv = (double)__ldg(val + e); }
-      const int m = (int)(end - e0 < 32 ? end - e0 : 32);
-#pragma unroll 4
-      for (int t = 0; t < m; ++t) {
-        const int j = __shfl_sync(0xffffffffu, jj, t);
-        const double v = __shfl_sync(0xffffffffu, vv, t);
-        const double* xr = X + (int64_t)j * ldx;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const int c = lane + 32 * r;
-          if (c < b) acc[r] = fma(v, __ldg(xr + c), acc[r]);
-        }
-      }
-    }
-    const double d = diag[i];
-    const double* xi = X + i * ldx;
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      const int c = lane + 32 * r;
-      if (c < b) Y[i * ldy + c] = fma(d, xi[c], acc[r]);
-    }
-  }
-}
-
-// One column panel Y[:, 0:bp] = (D + H_off) X[:, 0:bp], bp <= BP.  A warp handles one row; its
-// lanes form S = 32/BP entry slots of BP lanes (slot s takes entries s, s+S, ...), each lane owns
-// one column, and the slots are summed with shuffles at the end.  The launcher keeps the panel's
-// X columns (n * bp * 8 bytes) within the L2 budget so the per-entry gathers hit L2 while the
-// matrix streams from HBM once per panel.
+// Row-group SpMM, Y[:, 0:bp] = (D + H_off) X[:, 0:bp] for bp <= BP columns: a warp holds
+// G = 32/BP rows, each handled by a group of BP lanes that own one column each and walk the row's
+// entries together (the entry loads are broadcasts within the group and L1 hits across
+// consecutive entries), eight entries per iteration so each lane keeps eight vector-row gathers in
+// flight.  Entry loads are 16-byte (four columns, two or four values) after a scalar prologue to
+// 4-entry alignment.  The diagonal term reads X row xrow0 + i (a rank's row block of a sharded
+// matrix multiplies the gathered whole block); accum != 0 adds into Y instead (a later column
+// panel).
 template <int BP, typename VT>
-__global__ void __launch_bounds__(256) k_spmm_panel(int64_t n, const int64_t* __restrict__ rowptr,
-                                                    const int32_t* __restrict__ col,
-                                                    const VT* __restrict__ val,
-                                                    const double* __restrict__ diag,
-                                                    const double* __restrict__ X, int ldx, int bp,
-                                                    double* __restrict__ Y, int ldy) {
-  constexpr int S = 32 / BP;
-  const int lane = threadIdx.x & 31;
-  const int slot = lane / BP, cc = lane % BP;
-  const bool active = cc < bp;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
-       i += warps) {
-    double acc = 0.0;
-    const int64_t beg = rowptr[i], end = rowptr[i + 1];
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {
-      const int64_t e = e0 + lane;
-      int jj = 0;
-      double vv = 0.0;
-      if (e < end) { jj = __ldcs(col + e); vv = (double)__ldcs(val + e); }
-      const int m = (int)(end - e0 < 32 ? end - e0 : 32);
-#pragma unroll 4
-      for (int t = 0; t < m; t += S) {
-        const int src = t + slot;
-        const int j = __shfl_sync(0xffffffffu, jj, src & 31);
-        const double v = __shfl_sync(0xffffffffu, vv, src & 31);
-        if (active && src < m) acc = fma(v, __ldg(X + (int64_t)j * ldx + cc), acc);
-      }
-    }
-#pragma unroll
-    for (int o = BP; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (slot == 0 && active) Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
-  }
-}
-
-// Row-group form of the panel product: a warp holds G = 32/BP rows, each handled by a group of BP
-// lanes that own one column each and walk the row's entries together (the entry loads are
-// broadcasts within the group and L1 hits across consecutive entries), so the inner loop has no
-// shuffles: two cached loads, one gathered load and one FMA per entry.
-template <int BP, typename VT, bool CG, int U = 4>
 __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __restrict__ rowptr,
                                                    const int32_t* __restrict__ col,
                                                    const VT* __restrict__ val,
                                                    const double* __restrict__ diag,
                                                    const double* __restrict__ X, int ldx, int bp,
-                                                   double* __restrict__ Y, int ldy, int accum) {
+                                                   double* __restrict__ Y, int ldy, int accum,
+                                                   int64_t xrow0) {
   constexpr int G = 32 / BP;
   const int lane = threadIdx.x & 31;
   const int grp = lane / BP, cc = lane % BP;
@@ -190,199 +111,60 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
     const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
     double acc = 0.0;
     if (active && (!accum || end > beg)) {
-      auto gx = [&](int j) {
-        const double* xp = X + (int64_t)j * ldx + cc;
-        return CG ? __ldcg(xp) : __ldg(xp);
-      };
+      auto gx = [&](int j) { return __ldg(X + (int64_t)j * ldx + cc); };
       int64_t e = beg;
-      if constexpr (sizeof(VT) == 8) {
-        // entries four at a time: one 16-byte column load and two 16-byte value loads, each a
-        // broadcast within the group, after a scalar prologue to 4-entry alignment
-        for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
-        if constexpr (U == 8) {  // eight gathers in flight per lane
-          for (; e + 8 <= end; e += 8) {
-            const int4 ja = __ldg(reinterpret_cast<const int4*>(col + e));
-            const int4 jb = __ldg(reinterpret_cast<const int4*>(col + e + 4));
-            const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + e));
-            const double2 v23 = __ldg(reinterpret_cast<const double2*>(val + e + 2));
-            const double2 v45 = __ldg(reinterpret_cast<const double2*>(val + e + 4));
-            const double2 v67 = __ldg(reinterpret_cast<const double2*>(val + e + 6));
-            const double x0 = gx(ja.x), x1 = gx(ja.y), x2 = gx(ja.z), x3 = gx(ja.w);
-            const double x4 = gx(jb.x), x5 = gx(jb.y), x6 = gx(jb.z), x7 = gx(jb.w);
-            acc = fma(v01.x, x0, acc);
-            acc = fma(v01.y, x1, acc);
-            acc = fma(v23.x, x2, acc);
-            acc = fma(v23.y, x3, acc);
-            acc = fma(v45.x, x4, acc);
-            acc = fma(v45.y, x5, acc);
-            acc = fma(v67.x, x6, acc);
-            acc = fma(v67.y, x7, acc);
-          }
-        }
-        for (; e + 4 <= end; e += 4) {
-          const int4 j4 = __ldg(reinterpret_cast<const int4*>(col + e));
+      for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
+      for (; e + 8 <= end; e += 8) {
+        const int4 ja = __ldg(reinterpret_cast<const int4*>(col + e));
+        const int4 jb = __ldg(reinterpret_cast<const int4*>(col + e + 4));
+        double v[8];
+        if constexpr (sizeof(VT) == 8) {
           const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + e));
           const double2 v23 = __ldg(reinterpret_cast<const double2*>(val + e + 2));
-          const double x0 = gx(j4.x), x1 = gx(j4.y), x2 = gx(j4.z), x3 = gx(j4.w);
-          acc = fma((double)v01.x, x0, acc);
-          acc = fma((double)v01.y, x1, acc);
-          acc = fma((double)v23.x, x2, acc);
-          acc = fma((double)v23.y, x3, acc);
+          const double2 v45 = __ldg(reinterpret_cast<const double2*>(val + e + 4));
+          const double2 v67 = __ldg(reinterpret_cast<const double2*>(val + e + 6));
+          v[0] = v01.x; v[1] = v01.y; v[2] = v23.x; v[3] = v23.y;
+          v[4] = v45.x; v[5] = v45.y; v[6] = v67.x; v[7] = v67.y;
+        } else {
+          const float4 va = __ldg(reinterpret_cast<const float4*>(val + e));
+          const float4 vb = __ldg(reinterpret_cast<const float4*>(val + e + 4));
+          v[0] = va.x; v[1] = va.y; v[2] = va.z; v[3] = va.w;
+          v[4] = vb.x; v[5] = vb.y; v[6] = vb.z; v[7] = vb.w;
         }
-      } else {
-        // FP32 values: one 16-byte column load and one 16-byte value load per four entries
-        for (; e < end && (e & 3); ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
-        if constexpr (U == 8) {
-          for (; e + 8 <= end; e += 8) {
-            const int4 ja = __ldg(reinterpret_cast<const int4*>(col + e));
-            const int4 jb = __ldg(reinterpret_cast<const int4*>(col + e + 4));
-            const float4 va = __ldg(reinterpret_cast<const float4*>(val + e));
-            const float4 vb = __ldg(reinterpret_cast<const float4*>(val + e + 4));
-            const double x0 = gx(ja.x), x1 = gx(ja.y), x2 = gx(ja.z), x3 = gx(ja.w);
-            const double x4 = gx(jb.x), x5 = gx(jb.y), x6 = gx(jb.z), x7 = gx(jb.w);
-            acc = fma((double)va.x, x0, acc);
-            acc = fma((double)va.y, x1, acc);
-            acc = fma((double)va.z, x2, acc);
-            acc = fma((double)va.w, x3, acc);
-            acc = fma((double)vb.x, x4, acc);
-            acc = fma((double)vb.y, x5, acc);
-            acc = fma((double)vb.z, x6, acc);
-            acc = fma((double)vb.w, x7, acc);
-          }
-        }
-        for (; e + 4 <= end; e += 4) {
-          const int4 j4 = __ldg(reinterpret_cast<const int4*>(col + e));
-          const float4 v4 = __ldg(reinterpret_cast<const float4*>(val + e));
-          const double x0 = gx(j4.x), x1 = gx(j4.y), x2 = gx(j4.z), x3 = gx(j4.w);
-          acc = fma((double)v4.x, x0, acc);
-          acc = fma((double)v4.y, x1, acc);
-          acc = fma((double)v4.z, x2, acc);
-          acc = fma((double)v4.w, x3, acc);
-        }
+        const double x0 = gx(ja.x), x1 = gx(ja.y), x2 = gx(ja.z), x3 = gx(ja.w);
+        const double x4 = gx(jb.x), x5 = gx(jb.y), x6 = gx(jb.z), x7 = gx(jb.w);
+        acc = fma(v[0], x0, acc);
+        acc = fma(v[1], x1, acc);
+        acc = fma(v[2], x2, acc);
+        acc = fma(v[3], x3, acc);
+        acc = fma(v[4], x4, acc);
+        acc = fma(v[5], x5, acc);
+        acc = fma(v[6], x6, acc);
+        acc = fma(v[7], x7, acc);
       }
 #pragma unroll 4
       for (; e < end; ++e) acc = fma((double)__ldg(val + e), gx(__ldg(col + e)), acc);
-      if (accum) Y[i * ldy + cc] += acc;  // a later column panel: add this panel's entries
-      else Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
+      if (accum) Y[i * ldy + cc] += acc;
+      else Y[i * ldy + cc] = fma(diag[i], X[(xrow0 + i) * ldx + cc], acc);
     }
   }
 }
-
-// Row groups with cooperative entry loads: a warp holds G = 32/BP rows; a group of BP lanes loads
-// BP consecutive entries of its row in one coalesced access, then broadcasts them one by one with
-// width-BP shuffles while each lane gathers its own column.  Per entry the L1 sees one gathered
-// BP*8-byte segment plus 2/BP of a matrix-stream access.
-template <int BP, typename VT>
-__global__ void __launch_bounds__(256) k_spmm_rg(int64_t n, const int64_t* __restrict__ rowptr,
-                                                 const int32_t* __restrict__ col,
-                                                 const VT* __restrict__ val,
-                                                 const double* __restrict__ diag,
-                                                 const double* __restrict__ X, int ldx, int bp,
-                                                 double* __restrict__ Y, int ldy) {
-  constexpr int G = 32 / BP;
-  const int lane = threadIdx.x & 31;
-  const int grp = lane / BP, cc = lane % BP;
-  const unsigned gmask = (BP == 32) ? 0xffffffffu : (((1u << BP) - 1u) << (grp * BP));
-  const bool active = cc < bp;
-  const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5) * G;
-  for (int64_t i = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * G + grp;
-       i < n; i += stride) {
-    const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
-    double acc = 0.0;
-    for (int64_t e0 = beg; e0 < end; e0 += BP) {
-      const int64_t e = e0 + cc;
-      int jj = 0;
-      double vv = 0.0;
-      if (e < end) { jj = __ldcs(col + e); vv = (double)__ldcs(val + e); }
-      const int m = (int)(end - e0 < BP ? end - e0 : BP);
-#pragma unroll 8
-      for (int t = 0; t < m; ++t) {
-        const int j = __shfl_sync(gmask, jj, t, BP);
-        const double v = __shfl_sync(gmask, vv, t, BP);
-        if (active) acc = fma(v, __ldg(X + (int64_t)j * ldx + cc), acc);
-      }
-    }
-    if (active) Y[i * ldy + cc] = fma(diag[i], X[i * ldx + cc], acc);
-  }
-}
-
-// L2 budget for one panel of gathered vector columns (bytes); B200 has 126 MB of L2.
-constexpr double kSpmmL2Budget = 64e6;
 
 template <typename VT>
 void spmm_rows_launch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
                       const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
-                      int accum, cudaStream_t s) {
+                      int accum, int64_t xrow0, cudaStream_t s) {
   const int BP = b <= 8 ? 8 : (b <= 16 ? 16 : 32);
   const int gr = grid_for(n * BP, 256, 148 * 16);
-  // eight entries per iteration (eight gathers in flight per lane) by default; measured 11-14 %
-  // faster than four on the 380k- and 6.1M-state matrices.  VHCI_SPMM_UNROLL=4 selects four.
-  const char* ue = std::getenv("VHCI_SPMM_UNROLL");
-  const int u = ue ? std::atoi(ue) : 8;
   for (int c0 = 0; c0 < b; c0 += BP) {
     const int bp = std::min(BP, b - c0);
     note_launch();
-#define VHCI_ROWS(BPV, UV) k_spmm_rows<BPV, VT, false, UV><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, accum)
-#define VHCI_ROWS_U(BPV) do { if (u == 4) VHCI_ROWS(BPV, 4); else VHCI_ROWS(BPV, 8); } while (0)
-    if (BP == 32) VHCI_ROWS_U(32);
-    else if (BP == 16) VHCI_ROWS_U(16);
-    else VHCI_ROWS_U(8);
-#undef VHCI_ROWS_U
-#undef VHCI_ROWS
-  }
-}
-
-
-template <typename VT>
-void spmm_dispatch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
-                   const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
-                   cudaStream_t s) {
-  const int g = grid_for(n * 32, 256, 148 * 16);
-  // L2 holds whole 128-byte lines: a strided panel of BP columns occupies n * max(128, 8 BP)
-  // bytes, a compact one (ldx == b) n * 8 b bytes
-  const double rowbytes = (ldx == b) ? 8.0 * b : 128.0 * ((b + 15) / 16);
-  if ((double)n * rowbytes > kSpmmL2Budget || b <= 32) {
-    int BP = 32;
-    if (b <= 4) BP = 4;
-    else if (b <= 8) BP = 8;
-    else if (b <= 16) BP = 16;
-    else if (ldx != b && (double)n * 256.0 > kSpmmL2Budget) BP = 16;
-    const char* fe = std::getenv("VHCI_SPMM");
-    const std::string form = fe ? fe : "";
-    const bool slots = form == "slots";
-    for (int c0 = 0; c0 < b; c0 += BP) {
-      const int bp = std::min(BP, b - c0);
-      if (slots) {
-        if (BP == 4) BP = 8;
-        if (BP == 32) { note_launch(); k_spmm_panel<32, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else if (BP == 16) { note_launch(); k_spmm_panel<16, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else { note_launch(); k_spmm_panel<8, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-      } else if (form == "rg") {
-        const int gr = grid_for(n * BP, 256, 148 * 16);
-        if (BP == 32) { note_launch(); k_spmm_rg<32, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else if (BP == 16) { note_launch(); k_spmm_rg<16, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else if (BP == 8) { note_launch(); k_spmm_rg<8, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-        else { note_launch(); k_spmm_rg<4, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy); }
-      } else if (form == "rows_cg") {
-        if (BP == 4) BP = 8;
-        const int gr = grid_for(n * BP, 256, 148 * 16);
-        if (BP == 32) { note_launch(); k_spmm_rows<32, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0); }
-        else if (BP == 16) { note_launch(); k_spmm_rows<16, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0); }
-        else { note_launch(); k_spmm_rows<8, VT, true><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0); }
-      } else {
-        spmm_rows_launch<VT>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, 0, s);
-      }
-    }
-    return;
-  }
-  switch ((b + 31) / 32) {
-#define VHCI_SPMM_CASE(R) \
-  case R: note_launch(); k_spmm<R, VT><<<g, 256, 0, s>>>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy); break;
-    VHCI_SPMM_CASE(1) VHCI_SPMM_CASE(2) VHCI_SPMM_CASE(3) VHCI_SPMM_CASE(4)
-    VHCI_SPMM_CASE(5) VHCI_SPMM_CASE(6) VHCI_SPMM_CASE(7) VHCI_SPMM_CASE(8)
-    VHCI_SPMM_CASE(9) VHCI_SPMM_CASE(10) VHCI_SPMM_CASE(11) VHCI_SPMM_CASE(12)
-#undef VHCI_SPMM_CASE
-    default: break;
+    if (BP == 32)
+      k_spmm_rows<32, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, accum, xrow0);
+    else if (BP == 16)
+      k_spmm_rows<16, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, accum, xrow0);
+    else
+      k_spmm_rows<8, VT><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bp, Y + c0, ldy, accum, xrow0);
   }
 }
 
@@ -440,17 +222,18 @@ __global__ void k_fill_zero(double* p, int64_t n) {
 
 }  // namespace
 
-void hbuild_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
-                  int32_t* rowcnt, cudaStream_t s) {
+void hbuild_count(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L, HashView basis,
+                  ConnDev cd, int32_t* rowcnt, cudaStream_t s) {
   if (n <= 0) return;
-  VHCI_DISPATCH_W(L.W, hbuild_count_launch, keys, n, L, basis, cd, rowcnt, s);
+  VHCI_DISPATCH_W(L.W, hbuild_count_launch, keys, row0, n, L, basis, cd, rowcnt, s);
 }
 
-void hbuild_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
-                 const int64_t* rowptr, int32_t* col, double* val, float* valf, double* diag,
-                 cudaStream_t s) {
+void hbuild_fill(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L, HashView basis,
+                 ConnDev cd, const int64_t* rowptr, int32_t* col, double* val, float* valf,
+                 double* diag, cudaStream_t s) {
   if (n <= 0) return;
-  VHCI_DISPATCH_W(L.W, hbuild_fill_launch, keys, n, L, basis, cd, rowptr, col, val, valf, diag, s);
+  VHCI_DISPATCH_W(L.W, hbuild_fill_launch, keys, row0, n, L, basis, cd, rowptr, col, val, valf,
+                  diag, s);
 }
 
 // ---- column panels: the off-diagonal entries regrouped by column range -----------------------
@@ -536,20 +319,20 @@ void panel_fill(int64_t n, const int64_t* rowptr, const int32_t* col, const doub
 
 void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, const double* pval,
                  const float* pvalf, const double* diag, const double* X, int ldx, int b,
-                 double* Y, int ldy, cudaStream_t s) {
+                 double* Y, int ldy, int64_t xrow0, cudaStream_t s) {
   if (n <= 0 || b <= 0) return;
   for (int p = 0; p < P; ++p) {
-    if (pvalf) spmm_rows_launch<float>(n, prow + (int64_t)p * n, pcol, pvalf, diag, X, ldx, b, Y, ldy, p > 0, s);
-    else spmm_rows_launch<double>(n, prow + (int64_t)p * n, pcol, pval, diag, X, ldx, b, Y, ldy, p > 0, s);
+    if (pvalf) spmm_rows_launch<float>(n, prow + (int64_t)p * n, pcol, pvalf, diag, X, ldx, b, Y, ldy, p > 0, xrow0, s);
+    else spmm_rows_launch<double>(n, prow + (int64_t)p * n, pcol, pval, diag, X, ldx, b, Y, ldy, p > 0, xrow0, s);
   }
 }
 
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
           const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
-          int ldy, cudaStream_t s) {
+          int ldy, int64_t xrow0, cudaStream_t s) {
   if (n <= 0 || b <= 0) return;
-  if (valf) spmm_dispatch<float>(n, rowptr, col, valf, diag, X, ldx, b, Y, ldy, s);
-  else spmm_dispatch<double>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy, s);
+  if (valf) spmm_rows_launch<float>(n, rowptr, col, valf, diag, X, ldx, b, Y, ldy, 0, xrow0, s);
+  else spmm_rows_launch<double>(n, rowptr, col, val, diag, X, ldx, b, Y, ldy, 0, xrow0, s);
 }
 
 int residual_blocks(int64_t n) {

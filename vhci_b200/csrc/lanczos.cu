@@ -12,7 +12,12 @@
 //   * convergence: ||H x - theta x|| <= tol * max(eps^(2/3), |theta|) for the k wanted pairs,
 //     evaluated with explicit residuals at each restart (tol 1e-10 in the reference);
 //   * heat-bath iterations start from b random combinations of the previous Ritz vectors
-//     (zero-extended over the new states).
+//     (zero-extended over the new states);
+//   * on a sharded context every rank holds one contiguous row block of the Krylov basis (the
+//     rows of its Hamiltonian block): the vector block is all-gathered before each product, the
+//     projections' partial sums are all-reduced, the projected eigenproblem is solved on rank 0
+//     and broadcast, and the Ritz vectors are all-gathered at the end, so every rank holds them
+//     whole for the heat-bath selection.
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
@@ -79,11 +84,11 @@ void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std::vecto
 }
 
 struct LWork {
-  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc, gpart;
+  DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc, gpart, Xg, gtmp;
   void release(cudaStream_t s) {
     Q.release(s); HQ.release(s); T.release(s); Yw.release(s); theta.release(s); Xb.release(s);
     HXb.release(s); W.release(s); S.release(s); M.release(s); part.release(s); rn2.release(s);
-    Xc.release(s); gpart.release(s);
+    Xc.release(s); gpart.release(s); Xg.release(s); gtmp.release(s);
   }
 };
 
@@ -97,18 +102,34 @@ bool proj_blas() {
 }
 
 // Projections over the basis rows, on the FP64 tensor pipe (k_proj.cu).
-// C (M x P, column-major) = alpha A^T B + beta C, A n x M and B n x P row-major.
+// C (M x P, column-major) = alpha A^T B + beta C, A n x M and B n x P row-major.  On a sharded
+// context the n rows are this rank's block and the partial product is summed over the ranks
+// (beta must be 0 there).
 int gemm_gram(vhci_ctx* c, LWork& w, const double* A, int lda, const double* B, int ldb, int64_t n,
               int M, int P, double alpha, double beta, double* C, int ldc) {
   if (M <= 0 || P <= 0) return VHCI_OK;
+  const bool sh = is_sharded(c);
+  if (sh && beta != 0.0) return fail(c, VHCI_E_STATE, "accumulating projection on a sharded context");
+  double* out = C;
+  int ldo = ldc;
+  if (sh) {
+    VCK(w.gtmp.reserve((size_t)M * P, c->st));
+    out = w.gtmp.p;
+    ldo = M;
+  }
   if (proj_blas()) {
     VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, M, P, (int)n, &alpha, A, lda, B, ldb, &beta,
-                    C, ldc));
-    return VHCI_OK;
+                    out, ldo));
+  } else {
+    VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
+    if (!proj_gram(A, lda, B, ldb, n, M, P, alpha, beta, out, ldo, w.gpart.p, c->st))
+      return fail(c, VHCI_E_INPUT, "projection with more than 16 right-hand columns");
   }
-  VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
-  if (!proj_gram(A, lda, B, ldb, n, M, P, alpha, beta, C, ldc, w.gpart.p, c->st))
-    return fail(c, VHCI_E_INPUT, "projection with more than 16 right-hand columns");
+  if (sh) {
+    VTRY(comm_sum(c, out, (int64_t)M * P));
+    VCK(cudaMemcpy2DAsync(C, ldc * sizeof(double), out, M * sizeof(double), M * sizeof(double), P,
+                          cudaMemcpyDeviceToDevice, c->st));
+  }
   return VHCI_OK;
 }
 
@@ -180,16 +201,25 @@ int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb
   return VHCI_OK;
 }
 
-// Y = H X for a block: X is first copied to a compact n x b buffer so the SpMM gathers from a
-// small, L2-resident array instead of rows of the wide basis.
+// Y = H X for a block of the held rows: X is first copied to a compact rows x b buffer so the SpMM
+// gathers from a small, L2-resident array instead of rows of the wide basis; on a sharded context
+// the ranks' compact blocks (rblk rows each) are all-gathered into the whole vector block first.
 int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y, int ldy) {
   EventPair ev_e0e1;
   VCK(ev_e0e1.create());
   cudaEvent_t e0 = ev_e0e1.a, e1 = ev_e0e1.b;
-  VCK(w.Xc.reserve((size_t)c->n * b, c->st));
+  const int64_t nl = c->nrow, rb = c->rblk;
+  VCK(w.Xc.reserve((size_t)std::max(nl, rb) * b, c->st));
   VCK(cudaEventRecord(e0, c->st));
-  copy_cols(X, ldx, w.Xc.p, b, c->n, b, c->st);
-  spmm_h(c, w.Xc.p, b, b, Y, ldy);
+  copy_cols(X, ldx, w.Xc.p, b, nl, b, c->st);
+  const double* Xfull = w.Xc.p;
+  if (is_sharded(c)) {
+    if (nl < rb) fill_zero(w.Xc.p + (size_t)nl * b, (rb - nl) * (int64_t)b, c->st);
+    VCK(w.Xg.reserve((size_t)c->comm.nranks * rb * b, c->st));
+    VTRY(comm_gather(c, w.Xc.p, w.Xg.p, rb * b * (int64_t)sizeof(double)));
+    Xfull = w.Xg.p;
+  }
+  spmm_h(c, Xfull, b, b, Y, ldy);
   VCK(cudaEventRecord(e1, c->st));
   VCK(cudaEventSynchronize(e1));
   VCK(cudaGetLastError());
@@ -200,7 +230,39 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
   c->stats.spmm_cols += b;
   const int64_t sval = c->o.precision == 1 ? 4 : 8;
   c->stats.spmm_gather_bytes += c->nnz * (int64_t)b * 8;
-  c->stats.spmm_bytes += c->nnz * (sval + 4) + (c->n + 1) * 8 + c->n * 8 + 2 * c->n * (int64_t)b * 8;
+  c->stats.spmm_bytes += c->nnz * (sval + 4) + (nl + 1) * 8 + nl * 8 + 2 * nl * (int64_t)b * 8;
+  return VHCI_OK;
+}
+
+// Start vectors of the cold start: standard normal values drawn from the global (row, column)
+// index, so every rank draws the same values for its rows whatever the sharding.
+void random_rows(int64_t r0, int64_t rows, int b, std::vector<double>& out) {
+  out.resize((size_t)rows * b);
+  for (int64_t i = 0; i < rows; ++i)
+    for (int j = 0; j < b; ++j) {
+      const uint64_t key = ((uint64_t)(r0 + i) << 6) ^ (uint64_t)j;
+      const double u1 = ((mix64(2 * key + 0x9E3779B97F4A7C15ull) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+      const double u2 = ((mix64(2 * key + 1 + 0x9E3779B97F4A7C15ull) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+      out[(size_t)i * b + j] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    }
+}
+
+// Hands the Ritz block (this rank's rows, ld kk) to the context as its whole vectors: swapped in
+// on an unsharded context, all-gathered from the ranks' row blocks (rblk rows each; the buffer
+// holds at least that many) on a sharded one.
+int publish_ritz(vhci_ctx* c, DBuf<double>& Xb, int kk, int nk, const std::vector<double>& th) {
+  if (!is_sharded(c)) {
+    c->X.swap(Xb);
+  } else {
+    c->X.release(c->st);
+    VCK(c->X.reserve((size_t)c->comm.nranks * c->rblk * kk, c->st));
+    VTRY(comm_gather(c, Xb.p, c->X.p, c->rblk * kk * (int64_t)sizeof(double)));
+  }
+  c->ldx = kk;
+  c->nvec = nk;
+  c->x_rows = c->n;
+  c->E.assign(th.begin(), th.begin() + nk);
+  VCK(cudaStreamSynchronize(c->st));
   return VHCI_OK;
 }
 
@@ -227,32 +289,38 @@ static int lanczos_guard(int k) {
   return std::max(8, k * pct / 100);
 }
 
-// Working set of the block Lanczos for subspace factor `span`: Q and H Q (n x ld), the Ritz block
-// and its product (n x kk), the expansion block and its compact copy (n x b), in doubles.
-static double lanczos_bytes(int64_t n, int k, int span, int b) {
+// Working set of the block Lanczos over n states for subspace factor `span`, on a rank holding
+// `rows` of them: Q and H Q (rows x ld), the Ritz block and its product (rows x kk), the expansion
+// block and its compact copy (rows x b), and the gathered vector block (n x b), in doubles.
+static double lanczos_bytes(int64_t n, int64_t rows, int k, int span, int b) {
   const int kk = (int)std::min<int64_t>(n, k + lanczos_guard(k));
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   const int ld = (mmax + b + 15) / 16 * 16;
-  return 8.0 * (double)n * (2.0 * ld + 2.0 * kk + 2.0 * b);
+  return 8.0 * (double)rows * (2.0 * ld + 2.0 * kk + 2.0 * b) + (rows < n ? 8.0 * n * b : 0.0);
 }
 
 // Working set of the memory-lean variant: Q (n x ld, span 2), the expansion block, its product,
 // the compact copy (n x b each), the rotation chunk, and the output Ritz block (n x kk).
-static double lanczos_lean_bytes(int64_t n, int k, int b, int span = 2) {
+static double lanczos_lean_bytes(int64_t n, int64_t rows, int k, int b, int span = 2) {
   const int kk = (int)std::min<int64_t>(n, k + lanczos_guard(k));
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   const int ld = (mmax + b + 15) / 16 * 16;
-  return 8.0 * (double)n * (ld + 3.0 * b + kk) + 2.6e8;
+  return 8.0 * (double)rows * (ld + 3.0 * b + kk) + (rows < n ? 8.0 * n * (b + kk) : 0.0) + 2.6e8;
 }
 
+// Smallest eigensolver working set on this rank (the lean variant over the rows it will hold).
 double lanczos_min_bytes(vhci_ctx* c, int k) {
-  return lanczos_lean_bytes(c->n, k, lanczos_block(c->n)) + 1e9;
+  int64_t rows = c->n;
+  if (is_sharded(c) && !dense_path(c->n, k)) rows = (c->n + c->comm.nranks - 1) / c->comm.nranks;
+  return lanczos_lean_bytes(c->n, rows, k, lanczos_block(c->n)) + 1e9;
 }
 
 int block_lanczos_lean(vhci_ctx* c, int k);
 
 int block_lanczos(vhci_ctx* c, int k) {
   const int64_t n = c->n;
+  // rows held by this rank (all n unless sharded)
+  const int64_t nl = c->nrow, r0 = c->row0, rb = std::max(c->rblk, nl);
   cudaStream_t s = c->st;
   const int guard = lanczos_guard(k);
   const int kk = (int)std::min<int64_t>(n, k + guard);
@@ -264,7 +332,7 @@ int block_lanczos(vhci_ctx* c, int k) {
   if (const char* e = std::getenv("VHCI_LANCZOS_LEAN"))
     if (std::atoi(e) == 1) return block_lanczos_lean(c, k);
   if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) span = std::max(2, std::min(8, std::atoi(e)));
-  if (lanczos_bytes(n, k, span, b) + 1e9 > avail) return block_lanczos_lean(c, k);
+  if (lanczos_bytes(n, nl, k, span, b) + 1e9 > avail) return block_lanczos_lean(c, k);
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
@@ -273,18 +341,18 @@ int block_lanczos(vhci_ctx* c, int k) {
   const char* prof = std::getenv("VHCI_PROFILE");
   const int plevel = prof ? std::atoi(prof) : 0;
   LWork w;
-  VCK(w.Q.reserve((size_t)n * ld, s));
-  VCK(w.HQ.reserve((size_t)n * ld, s));
+  VCK(w.Q.reserve((size_t)nl * ld, s));
+  VCK(w.HQ.reserve((size_t)nl * ld, s));
   VCK(w.T.reserve((size_t)ld * ld, s));
   VCK(w.Yw.reserve((size_t)ld * ld, s));
   VCK(w.theta.reserve(ld, s));
-  VCK(w.Xb.reserve((size_t)n * kk, s));
-  VCK(w.HXb.reserve((size_t)n * kk, s));
-  VCK(w.W.reserve((size_t)n * b, s));
-  const int nblk = residual_blocks(n);
+  VCK(w.Xb.reserve((size_t)rb * kk, s));  // rblk rows: the block each rank gathers at the end
+  VCK(w.HXb.reserve((size_t)nl * kk, s));
+  VCK(w.W.reserve((size_t)nl * b, s));
+  const int nblk = residual_blocks(nl);
   VCK(w.part.reserve((size_t)nblk * kk, s));
   VCK(w.rn2.reserve(kk, s));
-  fill_zero(w.Q.p, n * (int64_t)ld, s);
+  fill_zero(w.Q.p, nl * (int64_t)ld, s);
   VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
 
   // ---- start block: random combinations of the previous Ritz vectors, else random vectors
@@ -306,17 +374,18 @@ int block_lanczos(vhci_ctx* c, int k) {
     DBuf<double> R;
     VCK(R.reserve(rnd.size(), s));
     VCK(h2d(c, R.p, rnd.data(), rnd.size() * sizeof(double)));
-    VTRY(gemm_rows(c, c->X.p, c->ldx, R.p, w0, (int)c->x_rows, w0, b, 1.0, 0.0, w.W.p, b));
-    if (c->x_rows < n) fill_zero(w.W.p + (size_t)c->x_rows * b, (n - c->x_rows) * (int64_t)b, s);
-    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    // this rank's rows of the previous vectors (held whole): rows r0 .. r0 + xr - 1
+    const int64_t xr = std::max<int64_t>(0, std::min<int64_t>(nl, c->x_rows - r0));
+    VTRY(gemm_rows(c, c->X.p + (size_t)r0 * c->ldx, c->ldx, R.p, w0, xr, w0, b, 1.0, 0.0, w.W.p, b));
+    if (xr < nl) fill_zero(w.W.p + (size_t)xr * b, (nl - xr) * (int64_t)b, s);
+    VTRY(svqb_small(c, w, nl, w.W.p, b, b, w.Q.p, ld, &p));
     VCK(cudaStreamSynchronize(s));
     R.release(s);
     if (p == 0) return fail(c, VHCI_E_NOT_CONVERGED, "empty start block");
   } else {
-    rnd.resize((size_t)n * b);
-    for (auto& x : rnd) x = nrand();
+    random_rows(r0, nl, b, rnd);
     VCK(h2d(c, w.W.p, rnd.data(), rnd.size() * sizeof(double)));
-    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    VTRY(svqb_small(c, w, nl, w.W.p, b, b, w.Q.p, ld, &p));
     if (p == 0) return fail(c, VHCI_E_NOT_CONVERGED, "empty start block");
   }
 
@@ -344,21 +413,21 @@ int block_lanczos(vhci_ctx* c, int k) {
       t0 = now();
       ++steps;
       // T[0:m+p, m:m+p] = Q^T (H Q_new)
-      VTRY(gemm_gram(c, w, w.Q.p, ld, w.HQ.p + m, ld, (int)n, m + p, p, 1.0, 0.0, w.T.p + (size_t)m * ld, ld));
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.HQ.p + m, ld, nl, m + p, p, 1.0, 0.0, w.T.p + (size_t)m * ld, ld));
       m += p;
       if (m + b > mmax || m >= n) {
         if (plevel) { cudaStreamSynchronize(s); t_orth += msince(t0); }
         break;
       }
       // next block: W = H Q_new - Q T[:, new]; second Gram-Schmidt pass; SVQB
-      copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, n, p, s);
-      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, (int)n, m, p, -1.0, 1.0, w.W.p, b));
+      copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
+      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)std::max(m, b) * p, s));
       bool second = true;
       if (kappa_max > 0) {
         // ||H q_c||^2 = ||T[:, c]||^2 + ||w_c||^2: the first pass removed the part of H q_c in
         // span(Q); a classical pass leaves an orthogonality error of about eps * ||H q_c|| / ||w_c||
-        VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, (int)n, p, p, 1.0, 0.0, w.S.p, p));
+        VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, nl, p, p, 1.0, 0.0, w.S.p, p));
         std::vector<double> G((size_t)p * p), Tc((size_t)m * p);
         VCK(d2h(c, G.data(), w.S.p, G.size() * sizeof(double)));
         VCK(cudaMemcpy2DAsync(Tc.data(), m * sizeof(double), w.T.p + (size_t)(m - p) * ld,
@@ -375,11 +444,11 @@ int block_lanczos(vhci_ctx* c, int k) {
         if (!second) ++skipped;
       }
       if (second) {
-        VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, (int)n, m, p, 1.0, 0.0, w.S.p, m));
-        VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, (int)n, m, p, -1.0, 1.0, w.W.p, b));
+        VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+        VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
       }
       int p2 = 0;
-      VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + m, ld, &p2));
+      VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + m, ld, &p2));
       t_orth += msince(t0);
       p = p2;
       if (p == 0) { exhausted = true; break; }
@@ -390,10 +459,14 @@ int block_lanczos(vhci_ctx* c, int k) {
     VCK(cudaMemcpy2DAsync(w.Yw.p, ld * sizeof(double), w.T.p, ld * sizeof(double),
                           m * sizeof(double), m, cudaMemcpyDeviceToDevice, s));
     VTRY(syevd_l(c, w.Yw.p, m, ld, w.theta.p));
+    // one projected solution for every rank: rank 0's
+    VTRY(comm_bcast0(c, w.Yw.p, (int64_t)ld * m));
+    VTRY(comm_bcast0(c, w.theta.p, m));
     const int nk = std::min(kk, m);
-    VTRY(gemm_rows(c, w.Q.p, ld, w.Yw.p, ld, (int)n, m, nk, 1.0, 0.0, w.Xb.p, kk));
-    VTRY(gemm_rows(c, w.HQ.p, ld, w.Yw.p, ld, (int)n, m, nk, 1.0, 0.0, w.HXb.p, kk));
-    residual_norms(w.Xb.p, w.HXb.p, n, kk, nk, w.theta.p, w.part.p, nblk, w.rn2.p, s);
+    VTRY(gemm_rows(c, w.Q.p, ld, w.Yw.p, ld, nl, m, nk, 1.0, 0.0, w.Xb.p, kk));
+    VTRY(gemm_rows(c, w.HQ.p, ld, w.Yw.p, ld, nl, m, nk, 1.0, 0.0, w.HXb.p, kk));
+    residual_norms(w.Xb.p, w.HXb.p, nl, kk, nk, w.theta.p, w.part.p, nblk, w.rn2.p, s);
+    VTRY(comm_sum(c, w.rn2.p, nk));
     VCK(d2h(c, th.data(), w.theta.p, nk * sizeof(double)));
     VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
     VCK(cudaStreamSynchronize(s));
@@ -415,26 +488,21 @@ int block_lanczos(vhci_ctx* c, int k) {
       if (plevel)
         std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d (second pass skipped %d) ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
                      (long long)n, k, b, cyc + 1, steps, skipped, t_spmm, t_orth, t_rr, msince(t_start));
-      c->X.swap(w.Xb);  // hand the Ritz block over; the old X buffer is released with w
-      c->ldx = kk;
-      c->nvec = nk;
-      c->x_rows = n;
-      c->E.assign(th.begin(), th.begin() + nk);
-      VCK(cudaStreamSynchronize(s));
+      VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
     }
     // ---- thick restart: pending block from the last expansion, then keep the Ritz block
     t0 = now();
-    copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, n, p, s);
-    VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, (int)n, m, p, -1.0, 1.0, w.W.p, b));
+    copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
+    VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
     VCK(w.S.reserve((size_t)m * p, s));
-    VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, (int)n, m, p, 1.0, 0.0, w.S.p, m));
-    VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, (int)n, m, p, -1.0, 1.0, w.W.p, b));
-    copy_cols(w.Xb.p, kk, w.Q.p, ld, n, nk, s);
-    copy_cols(w.HXb.p, kk, w.HQ.p, ld, n, nk, s);
+    VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+    VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
+    copy_cols(w.Xb.p, kk, w.Q.p, ld, nl, nk, s);
+    copy_cols(w.HXb.p, kk, w.HQ.p, ld, nl, nk, s);
     int p2 = 0;
-    VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + nk, ld, &p2));
+    VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + nk, ld, &p2));
     std::vector<double> Th((size_t)ld * nk, 0.0);
     for (int j = 0; j < nk; ++j) Th[(size_t)j * ld + j] = th[j];
     VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
@@ -446,12 +514,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       exhausted = true;
     }
     if (exhausted) {
-      c->X.swap(w.Xb);  // hand the Ritz block over; the old X buffer is released with w
-      c->ldx = kk;
-      c->nvec = nk;
-      c->x_rows = n;
-      c->E.assign(th.begin(), th.begin() + nk);
-      VCK(cudaStreamSynchronize(s));
+      VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
     }
@@ -472,6 +535,7 @@ int block_lanczos(vhci_ctx* c, int k) {
 //     with explicit residuals H x - theta x, block by block, before returning.
 int block_lanczos_lean(vhci_ctx* c, int k) {
   const int64_t n = c->n;
+  const int64_t nl = c->nrow, r0 = c->row0, rb = std::max(c->rblk, nl);
   cudaStream_t s = c->st;
   const int guard = lanczos_guard(k);
   const int kk = (int)std::min<int64_t>(n, k + guard);
@@ -484,18 +548,18 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
   const char* prof = std::getenv("VHCI_PROFILE");
   const int plevel = prof ? std::atoi(prof) : 0;
   const int64_t chunk = std::max<int64_t>(1024, (int64_t)(2.5e8 / (8.0 * kk)));
-  LWork w;  // Q, T, Yw, theta, W (pending block), HQ (n x b product), Xb (rotation chunk)
-  VCK(w.Q.reserve((size_t)n * ld, s));
-  VCK(w.HQ.reserve((size_t)n * b, s));
-  VCK(w.W.reserve((size_t)n * b, s));
-  VCK(w.Xb.reserve((size_t)std::min<int64_t>(n, chunk) * kk, s));
+  LWork w;  // Q, T, Yw, theta, W (pending block), HQ (rows x b product), Xb (rotation chunk)
+  VCK(w.Q.reserve((size_t)nl * ld, s));
+  VCK(w.HQ.reserve((size_t)nl * b, s));
+  VCK(w.W.reserve((size_t)nl * b, s));
+  VCK(w.Xb.reserve((size_t)std::max<int64_t>(1, std::min<int64_t>(nl, chunk)) * kk, s));
   VCK(w.T.reserve((size_t)ld * ld, s));
   VCK(w.Yw.reserve((size_t)ld * ld, s));
   VCK(w.theta.reserve(ld, s));
-  const int nblk = residual_blocks(n);
+  const int nblk = residual_blocks(nl);
   VCK(w.part.reserve((size_t)nblk * b, s));
   VCK(w.rn2.reserve(kk, s));
-  fill_zero(w.Q.p, n * (int64_t)ld, s);
+  fill_zero(w.Q.p, nl * (int64_t)ld, s);
   VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
 
   // start block, as in block_lanczos
@@ -514,16 +578,16 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
     DBuf<double> R;
     VCK(R.reserve(rnd.size(), s));
     VCK(h2d(c, R.p, rnd.data(), rnd.size() * sizeof(double)));
-    VTRY(gemm_rows(c, c->X.p, c->ldx, R.p, w0, (int)c->x_rows, w0, b, 1.0, 0.0, w.W.p, b));
-    if (c->x_rows < n) fill_zero(w.W.p + (size_t)c->x_rows * b, (n - c->x_rows) * (int64_t)b, s);
-    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    const int64_t xr = std::max<int64_t>(0, std::min<int64_t>(nl, c->x_rows - r0));
+    VTRY(gemm_rows(c, c->X.p + (size_t)r0 * c->ldx, c->ldx, R.p, w0, xr, w0, b, 1.0, 0.0, w.W.p, b));
+    if (xr < nl) fill_zero(w.W.p + (size_t)xr * b, (nl - xr) * (int64_t)b, s);
+    VTRY(svqb_small(c, w, nl, w.W.p, b, b, w.Q.p, ld, &p));
     VCK(cudaStreamSynchronize(s));
     R.release(s);
   } else {
-    rnd.resize((size_t)n * b);
-    for (auto& x : rnd) x = nrand();
+    random_rows(r0, nl, b, rnd);
     VCK(h2d(c, w.W.p, rnd.data(), rnd.size() * sizeof(double)));
-    VTRY(svqb_small(c, w, n, w.W.p, b, b, w.Q.p, ld, &p));
+    VTRY(svqb_small(c, w, nl, w.W.p, b, b, w.Q.p, ld, &p));
   }
   if (p == 0) return fail(c, VHCI_E_NOT_CONVERGED, "empty start block");
   // the previous Ritz block is no longer needed: its memory goes to the Krylov basis
@@ -531,19 +595,32 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
   c->nvec = 0;
   c->x_rows = 0;
 
+  std::vector<double> th(ld), rn(kk), G, Yl;
   // Q[:, 0:nk] = Q[:, 0:m] Y[0:m, 0:nk], in row chunks through w.Xb
   auto rotate = [&](int mm, int nk) -> int {
-    for (int64_t r0 = 0; r0 < n; r0 += chunk) {
-      const int64_t rows = std::min(chunk, n - r0);
-      VTRY(gemm_rows(c, w.Q.p + (size_t)r0 * ld, ld, w.Yw.p, ld, (int)rows, mm, nk, 1.0, 0.0, w.Xb.p, nk));
-      VCK(cudaMemcpy2DAsync(w.Q.p + (size_t)r0 * ld, ld * sizeof(double), w.Xb.p,
+    for (int64_t q0 = 0; q0 < nl; q0 += chunk) {
+      const int64_t rows = std::min(chunk, nl - q0);
+      VTRY(gemm_rows(c, w.Q.p + (size_t)q0 * ld, ld, w.Yw.p, ld, rows, mm, nk, 1.0, 0.0, w.Xb.p, nk));
+      VCK(cudaMemcpy2DAsync(w.Q.p + (size_t)q0 * ld, ld * sizeof(double), w.Xb.p,
                             nk * sizeof(double), nk * sizeof(double), rows,
                             cudaMemcpyDeviceToDevice, s));
     }
     return VHCI_OK;
   };
+  // the Ritz vectors, rotated into Q[:, 0:nk], become the context's vectors
+  auto finish = [&](int nk) -> int {
+    w.HQ.release(s);
+    w.W.release(s);
+    w.Xb.release(s);
+    DBuf<double> out;
+    VCK(out.reserve((size_t)rb * kk, s));
+    copy_cols(w.Q.p, ld, out.p, kk, nl, nk, s);
+    VTRY(publish_ritz(c, out, kk, nk, th));
+    out.release(s);
+    w.release(s);
+    return VHCI_OK;
+  };
 
-  std::vector<double> th(ld), rn(kk), G, Yl;
   const int maxcyc = c->o.eig_maxit > 0 ? c->o.eig_maxit : 1000;
   auto t_start = std::chrono::steady_clock::now();
   int steps = 0;
@@ -553,18 +630,18 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
     while (true) {
       VTRY(apply_h_l(c, w, w.Q.p + m, ld, p, w.HQ.p, b));
       ++steps;
-      VTRY(gemm_gram(c, w, w.Q.p, ld, w.HQ.p, b, (int)n, m + p, p, 1.0, 0.0, w.T.p + (size_t)m * ld, ld));
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.HQ.p, b, nl, m + p, p, 1.0, 0.0, w.T.p + (size_t)m * ld, ld));
       m += p;
       plast = p;
       // pending block W = H Q_new - Q T[:, new], second Gram-Schmidt pass
-      VCK(cudaMemcpyAsync(w.W.p, w.HQ.p, (size_t)n * b * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, (int)n, m, p, -1.0, 1.0, w.W.p, b));
+      VCK(cudaMemcpyAsync(w.W.p, w.HQ.p, (size_t)nl * b * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)m * p, s));
-      VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, (int)n, m, p, 1.0, 0.0, w.S.p, m));
-      VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, (int)n, m, p, -1.0, 1.0, w.W.p, b));
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
       if (m + b > mmax || m >= n) break;
       int p2 = 0;
-      VTRY(svqb_small(c, w, n, w.W.p, b, p, w.Q.p + m, ld, &p2));
+      VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + m, ld, &p2));
       if (p2 == 0) { exhausted = true; break; }
       p = p2;
     }
@@ -573,12 +650,14 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
     VCK(cudaMemcpy2DAsync(w.Yw.p, ld * sizeof(double), w.T.p, ld * sizeof(double),
                           m * sizeof(double), m, cudaMemcpyDeviceToDevice, s));
     VTRY(syevd_l(c, w.Yw.p, m, ld, w.theta.p));
+    VTRY(comm_bcast0(c, w.Yw.p, (int64_t)ld * m));
+    VTRY(comm_bcast0(c, w.theta.p, m));
     const int nk = std::min(kk, m);
     const int keff = std::min(k, nk);
     VCK(d2h(c, th.data(), w.theta.p, m * sizeof(double)));
     // residual estimates from the pending block: G = W^T W (plast x plast), Y's last-block rows
     VCK(w.S.reserve((size_t)plast * plast, s));
-    VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, (int)n, plast, plast, 1.0, 0.0, w.S.p, plast));
+    VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, nl, plast, plast, 1.0, 0.0, w.S.p, plast));
     G.resize((size_t)plast * plast);
     Yl.resize((size_t)plast * nk);
     VCK(d2h(c, G.data(), w.S.p, G.size() * sizeof(double)));
@@ -609,7 +688,8 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
         const int bw = std::min(b, keff - j0);
         // compact copy (w.Xc) and product both n x bw
         VTRY(apply_h_l(c, w, w.Q.p + j0, ld, bw, w.HQ.p, bw));
-        residual_norms(w.Xc.p, w.HQ.p, n, bw, bw, w.theta.p + j0, w.part.p, nblk, w.rn2.p + j0, s);
+        residual_norms(w.Xc.p, w.HQ.p, nl, bw, bw, w.theta.p + j0, w.part.p, nblk, w.rn2.p + j0, s);
+        VTRY(comm_sum(c, w.rn2.p + j0, bw));
         VCK(d2h(c, rn.data() + j0, w.rn2.p + j0, bw * sizeof(double)));
         VCK(cudaStreamSynchronize(s));
         for (int j = j0; j < j0 + bw; ++j)
@@ -621,39 +701,18 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
         std::fprintf(stderr, "lanczos(lean) n %lld k %d b %d span %d cycles %d steps %d ms total %.1f\n",
                      (long long)n, k, b, span, cyc + 1, steps,
                      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
-      w.HQ.release(s);
-      w.W.release(s);
-      w.Xb.release(s);
-      VCK(c->X.reserve((size_t)n * kk, s));
-      copy_cols(w.Q.p, ld, c->X.p, kk, n, nk, s);
-      c->ldx = kk;
-      c->nvec = nk;
-      c->x_rows = n;
-      c->E.assign(th.begin(), th.begin() + nk);
-      VCK(cudaStreamSynchronize(s));
-      w.release(s);
-      return VHCI_OK;
+      return finish(nk);
     }
     // thick restart: kept Ritz vectors Q[:, 0:nk] (already rotated), then the pending block
     int p2 = 0;
-    VTRY(svqb_small(c, w, n, w.W.p, b, plast, w.Q.p + nk, ld, &p2));
+    VTRY(svqb_small(c, w, nl, w.W.p, b, plast, w.Q.p + nk, ld, &p2));
     std::vector<double> Th((size_t)ld * nk, 0.0);
     for (int j = 0; j < nk; ++j) Th[(size_t)j * ld + j] = th[j];
     VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
     VCK(h2d(c, w.T.p, Th.data(), Th.size() * sizeof(double)));
     m = nk;
     p = p2;
-    if (p == 0) {  // invariant: the rotated block is exact
-      VCK(c->X.reserve((size_t)n * kk, s));
-      copy_cols(w.Q.p, ld, c->X.p, kk, n, nk, s);
-      c->ldx = kk;
-      c->nvec = nk;
-      c->x_rows = n;
-      c->E.assign(th.begin(), th.begin() + nk);
-      VCK(cudaStreamSynchronize(s));
-      w.release(s);
-      return VHCI_OK;
-    }
+    if (p == 0) return finish(nk);  // invariant: the rotated block is exact
   }
   w.release(s);
   return fail(c, VHCI_E_NOT_CONVERGED, "Error: Eigenvalues did not converge.");

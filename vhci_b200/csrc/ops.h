@@ -107,11 +107,12 @@ void radix_sort_keys(uint64_t* keys, uint64_t* alt, int64_t n, int W, int nbits,
                      cudaStream_t s);
 
 // ---- Hamiltonian (k_ham.cu) ----
-void hbuild_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
-                  int32_t* rowcnt, cudaStream_t s);
-void hbuild_fill(const uint64_t* keys, int64_t n, KeyLayout L, HashView basis, ConnDev cd,
-                 const int64_t* rowptr, int32_t* col, double* val, float* valf, double* diag,
-                 cudaStream_t s);
+// Rows row0 .. row0 + n - 1 of the Hamiltonian (rowcnt, rowptr, diag indexed from row0).
+void hbuild_count(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L, HashView basis,
+                  ConnDev cd, int32_t* rowcnt, cudaStream_t s);
+void hbuild_fill(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L, HashView basis,
+                 ConnDev cd, const int64_t* rowptr, int32_t* col, double* val, float* valf,
+                 double* diag, cudaStream_t s);
 // Column panels of the off-diagonal CSR (at most kMaxPanels): entries of panel p (columns
 // [p cw, (p+1) cw)) for row i at [prow[p n + i], prow[p n + i + 1]).
 constexpr int kMaxPanels = 64;
@@ -120,13 +121,15 @@ void panel_count(int64_t n, const int64_t* rowptr, const int32_t* col, int64_t c
 void panel_fill(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
                 const float* valf, int64_t cw, int P, const int64_t* prow, int32_t* pcol,
                 double* pval, float* pvalf, cudaStream_t s);
+// Y[:, 0:b] = H X[:, 0:b] for the n rows of a CSR (or column-panelled) matrix of FP64 or FP32
+// off-diagonal values plus the FP64 diagonal; the diagonal term of row i multiplies X row
+// xrow0 + i (0 unless the rows are one rank's block of a sharded matrix).
 void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, const double* pval,
                  const float* pvalf, const double* diag, const double* X, int ldx, int b,
-                 double* Y, int ldy, cudaStream_t s);
-// Y[:, 0:b] = H X[:, 0:b] with H = diag + off-diagonal CSR (FP64 or FP32 values).
+                 double* Y, int ldy, int64_t xrow0, cudaStream_t s);
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
           const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
-          int ldy, cudaStream_t s);
+          int ldy, int64_t xrow0, cudaStream_t s);
 // ---- eigensolver helpers ----
 // rn2[c] (c < kk) = sum_i (HX[i,c] - theta[c] X[i,c])^2   (block partials reduced on device)
 void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,

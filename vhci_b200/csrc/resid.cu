@@ -102,7 +102,8 @@ using namespace vhci;
 extern "C" vhci_status vhci_residual_norms(vhci_ctx* c, const double* X, const double* theta,
                                            double* rnorm, int k) {
   if (!c || !X || !theta || !rnorm || k <= 0) return VHCI_E_INPUT;
-  if (!c->h_valid) VTRY(build_h(c));
+  if (is_sharded(c)) return fail(c, VHCI_E_STATE, "vhci_residual_norms on a sharded context");
+  if (!c->h_valid || c->h_rows) VTRY(build_h(c, true));
   const int64_t n = c->n;
   std::vector<double> h((size_t)n * k);
   for (int64_t i = 0; i < n; ++i)
@@ -176,6 +177,8 @@ extern "C" vhci_status vhci_residual_norms_noalloc(vhci_ctx* c, const double* X_
     return fail(c, VHCI_E_STATE,
                 "vhci_residual_norms_noalloc: the Hamiltonian is not built; call vhci_build_h "
                 "first (building it allocates, this call does not)");
+  if (c->h_rows)
+    return fail(c, VHCI_E_STATE, "vhci_residual_norms_noalloc: the Hamiltonian is sharded");
   const int dev = c->o.device;
   if (dev < 0 || dev >= 128) return fail(c, VHCI_E_CUDA, "device ordinal out of range");
   DeviceGuard guard;
