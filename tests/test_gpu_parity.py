@@ -146,12 +146,10 @@ def test_davidson_end_to_end_workload0(api):
     assert r["n_basis"] == g["log"]["final_basis"]
 
 
-@pytest.mark.parametrize("form", ["rg", "rows", "slots"])
 @pytest.mark.parametrize("b", [1, 5, 8, 13, 16, 31, 40, 97])
-def test_spmm_matches_csr_product(api, b, form, monkeypatch):
-    """H X on the device (both panel kernels, all panel widths) against the CSR product of the
-    same matrix."""
-    monkeypatch.setenv("VHCI_SPMM", form)
+def test_spmm_matches_csr_product(api, b):
+    """H X on the device (every column-panel width of the row-group kernel) against the CSR
+    product of the same matrix."""
     g = load_golden("syn_m8_sextic_pt2")
     o = O.Oracle(g["input"])
     w, C = _oracle_first_step(o)
