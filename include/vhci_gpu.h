@@ -60,6 +60,8 @@ typedef struct {
                           basis past this fails with VHCI_E_LIMIT before building H             */
   int64_t max_pert;    /* 0 = no limit; else PT2 fails with VHCI_E_LIMIT when the screened
                           perturber space is larger, before the perturber Hamiltonian is built  */
+  int stream_priority; /* priority of the context's CUDA stream (cudaStreamCreateWithPriority:
+                          lower numbers run first, clamped to the device's range; 0 = default)  */
 } vhci_opts;
 
 /* Problem description in memory (the content of a reference input file, Input_Reader.cpp). */
@@ -268,6 +270,9 @@ typedef struct {
   double reserve_bytes;            /* free device memory required to admit (default 8e9)        */
   int max_states;                  /* energies stored per request (default 256)                 */
   int64_t max_basis, max_pert;     /* per-request size limits, as in vhci_opts (default 0: none)  */
+  int fifo_priority;               /* 1 (default): a request admitted while others run gets a lower
+                                      stream priority than all of them, so the earliest requests
+                                      finish about as fast as alone and later ones fill the gaps  */
 } vhci_serve_opts;
 
 typedef struct {

@@ -45,7 +45,7 @@ class Opts(ctypes.Structure):
                 ("eig_maxit", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("host_threads", ctypes.c_int), ("pt2_chunk", ctypes.c_int64),
                 ("structural_nnz", ctypes.c_int), ("max_basis", ctypes.c_int64),
-                ("max_pert", ctypes.c_int64)]
+                ("max_pert", ctypes.c_int64), ("stream_priority", ctypes.c_int)]
 
 
 class Problem(ctypes.Structure):
@@ -90,7 +90,8 @@ class Request(ctypes.Structure):
 class ServeOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int),
                 ("reserve_bytes", ctypes.c_double), ("max_states", ctypes.c_int),
-                ("max_basis", ctypes.c_int64), ("max_pert", ctypes.c_int64)]
+                ("max_basis", ctypes.c_int64), ("max_pert", ctypes.c_int64),
+                ("fifo_priority", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -432,7 +433,8 @@ def _problem_struct(p: dict):
 
 
 def serve(requests, slots: int = 8, reserve_bytes: float = 8e9, device: int = 0,
-          max_states: int = 256, max_basis: int = 0, max_pert: int = 0):
+          max_states: int = 256, max_basis: int = 0, max_pert: int = 0,
+          fifo_priority: bool = True):
     """Run many independent solves on one GPU with continuous batching (vhci_serve).
     `requests` is a list of (input_path, arrival_seconds).  Returns (summary dict, list of
     per-request dicts: status, energies, basis size, |P|, arrival/admit/done times, message)."""
@@ -449,6 +451,7 @@ def serve(requests, slots: int = 8, reserve_bytes: float = 8e9, device: int = 0,
     lib().vhci_default_serve_opts(ctypes.byref(so))
     so.device, so.slots, so.reserve_bytes, so.max_states = device, slots, reserve_bytes, max_states
     so.max_basis, so.max_pert = max_basis, max_pert
+    so.fifo_priority = 1 if fifo_priority else 0
     res = (Result * n)()
     E = np.zeros(n * max_states)
     summ = ServeSummary()

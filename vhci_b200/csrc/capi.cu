@@ -89,6 +89,7 @@ static int upload(vhci_ctx* c, DBuf<T>& b, const std::vector<T>& h) {
 namespace {
 struct HandleSet {
   int device;
+  int priority;
   cudaStream_t st;
   cublasHandle_t blas;
   cusolverDnHandle_t sol;
@@ -97,11 +98,21 @@ std::mutex g_handle_mu;
 std::vector<HandleSet> g_handle_pool;
 }  // namespace
 
+// Stream priority of a context: the requested value clamped to the device's range.
+static int clamped_priority(int want) {
+  if (want == 0) return 0;
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) return 0;
+  return std::max(greatest, std::min(least, want));
+}
+
 static int acquire_handles(vhci_ctx* c) {
+  const int prio = clamped_priority(c->o.stream_priority);
+  c->o.stream_priority = prio;
   {
     std::lock_guard<std::mutex> lk(g_handle_mu);
     for (size_t i = 0; i < g_handle_pool.size(); ++i)
-      if (g_handle_pool[i].device == c->o.device) {
+      if (g_handle_pool[i].device == c->o.device && g_handle_pool[i].priority == prio) {
         c->st = g_handle_pool[i].st;
         c->blas = g_handle_pool[i].blas;
         c->sol = g_handle_pool[i].sol;
@@ -109,7 +120,7 @@ static int acquire_handles(vhci_ctx* c) {
         return VHCI_OK;
       }
   }
-  VCK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  VCK(cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio));
   VBL(cublasCreate(&c->blas));
   VBL(cublasSetStream(c->blas, c->st));
   VBL(cusolverDnCreate(&c->sol));
@@ -126,7 +137,7 @@ static void release_handles(vhci_ctx* c) {
   }
   cudaStreamSynchronize(c->st);
   std::lock_guard<std::mutex> lk(g_handle_mu);
-  g_handle_pool.push_back(HandleSet{c->o.device, c->st, c->blas, c->sol});
+  g_handle_pool.push_back(HandleSet{c->o.device, c->o.stream_priority, c->st, c->blas, c->sol});
 }
 
 // Layout-dependent tables (packed key deltas, ladder factors) and the layout-free ones.

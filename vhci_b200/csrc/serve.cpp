@@ -3,7 +3,9 @@
 // has arrived, a slot is free and the device's free memory exceeds the reserve.  Each admitted
 // request runs on its own context (own CUDA stream, cuBLAS/cuSOLVER handles and buffers), so the
 // kernels of concurrent requests overlap on the device; a slot that finishes takes the next
-// arrived request at once.  A request that runs out of device memory releases everything and
+// arrived request at once.  A request admitted while others run gets a lower CUDA stream priority
+// than they have, so the block scheduler serves the earliest requests first (they finish about as
+// fast as alone) and later ones run in the gaps.  A request that runs out of device memory releases everything and
 // goes back to waiting until another request has finished (it fails only if it runs out of memory
 // with nothing else running).  Optional per-request size limits reject a request whose basis or
 // perturber space would grow past them, before the step that would build it.  There is no
@@ -48,12 +50,13 @@ struct Server {
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
 
-void solve_one(Server& S, int r, int worker) {
+void solve_one(Server& S, int r, int worker, int priority) {
   const vhci_request& q = S.reqs[r];
   vhci_result& out = S.res[r];
   vhci_opts o;
   vhci_default_opts(&o);
   o.device = S.so.device;
+  o.stream_priority = priority;
   o.max_basis = S.so.max_basis;
   o.max_pert = S.so.max_pert;
   out.n_energies = 0;
@@ -102,8 +105,11 @@ double available_bytes(int device) {
 
 void worker_loop(Server& S, int worker) {
   cudaSetDevice(S.so.device);
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
   for (;;) {
     int r = -1;
+    int priority = 0;
     {
       std::unique_lock<std::mutex> lk(S.mu);
       for (;;) {
@@ -117,6 +123,9 @@ void worker_loop(Server& S, int worker) {
             (S.running == 0 || available_bytes(S.so.device) >= S.so.reserve_bytes)) {
           r = S.ready.front();
           S.ready.pop_front();
+          // arrival-order priority: below every request already running (lower numbers run
+          // first; the device has least - greatest + 1 levels, the last one is shared)
+          if (S.so.fifo_priority) priority = std::min(least, greatest + S.running);
           ++S.running;
           S.in_flight_peak = std::max(S.in_flight_peak, S.running);
           S.res[r].t_admit = t;
@@ -132,7 +141,7 @@ void worker_loop(Server& S, int worker) {
     S.res[r].retries = 0;
     int solo_done = -1;  // S.done when this request last retried while all others were waiting
     for (;;) {
-      solve_one(S, r, worker);
+      solve_one(S, r, worker, priority);
       if (S.res[r].status != VHCI_E_OOM) break;
       // out of device memory (its buffers are already released): wait until another request
       // finishes; when every running request is waiting, the lowest-numbered one retries once,
@@ -173,6 +182,7 @@ void vhci_default_serve_opts(vhci_serve_opts* so) {
   so->max_states = 256;
   so->max_basis = 0;
   so->max_pert = 0;
+  so->fifo_priority = 1;
 }
 
 vhci_status vhci_serve(const vhci_request* reqs, int nreq, const vhci_serve_opts* so,
