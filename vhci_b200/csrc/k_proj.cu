@@ -2,18 +2,25 @@
 // block orthonormalisation and the Rayleigh-Ritz rotations).  The reference eigensolver (Spectra's
 // implicitly restarted Lanczos, Ham.cpp:347-370) does these with Eigen's dense products; here they
 // are skinny products over the whole basis, written for B200's FP64 tensor pipe (DMMA,
-// mma.sync.m8n8k4.f64), with operand tiles staged in shared memory by cp.async:
+// mma.sync.m8n8k4.f64).  Both read the tall operand once, straight from global memory into the
+// DMMA fragment registers (each lane's fragment element is 8 bytes of a 32-byte row segment, so
+// the sectors are fully used), with several k-steps of loads in flight per lane and 32 warps per
+// SM; the main loops have no block-wide barriers:
 //
-//   proj_gram:  C = alpha * A^T B + beta * C   A: n x M, B: n x P (row-major), C: M x P col-major
-//               (P <= 16; M in slabs of 1024).  The n rows are split over the blocks; each block
-//               keeps its partial slab x P product in registers (one warp per group of 8-row
-//               tiles of C) and writes it to scratch; a second kernel sums the partials in block
-//               order, so the result does not depend on scheduling.
+//   proj_gram:  C = alpha * A^T B + beta * C   A: n x M, B: n x P (row-major), C: M x P col-major,
+//               P <= 16.  A persistent grid splits the n rows over the blocks; each warp keeps
+//               the partial products of its 8-row tiles of C in registers; the blocks' partials
+//               go to scratch and a second kernel sums them in block order, so the result does not
+//               depend on scheduling.
 //   proj_rows:  Out = alpha * A S + beta * Out   A: n x M row-major, S: M x P col-major,
-//               Out: n x P row-major.  A block owns 64 rows of A (one 8-row tile per warp) and
-//               streams the M dimension through shared memory in chunks of 32.
+//               Out: n x P row-major.  Each block holds a 16-column slab of S in shared memory
+//               and its warps stream 8-row tiles of A.
+//
+// Fragment layouts of m8n8k4 (row.col): A[m][k] sits in lane 4 m + k, B[k][n] in lane 4 n + k,
+// D[m][n] in lane 4 m + n / 2 (element n % 2).
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include "ops.h"
 
@@ -27,120 +34,75 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void cp16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+constexpr int kThreads = 1024;      // proj_rows: 32 warps, one block per SM
+constexpr int kBlocks = 148;
+constexpr int kUnroll = 4;          // proj_rows: k-steps of loads issued ahead
+constexpr int kGramThreads = 512;   // proj_gram: 16 warps with up to 128 registers each
+constexpr int kGramWarps = kGramThreads / 32;
+constexpr int kGramTiles = 6;       // 8-row tiles of C per warp: a slab of 16 x 6 x 8 = 768 rows
+constexpr int kGramSlab = kGramWarps * kGramTiles * 8;
+constexpr int kGramUnroll = 2;
 
-constexpr int kThreads = 256;
-constexpr int kGramRows = 16;   // rows per shared-memory stage (four k-steps of 4)
-constexpr int kGramMT = 16;     // 8-row tiles of C per warp: a slab of 8 warps x 16 x 8 = 1024
-constexpr int kGramSlab = 8 * kGramMT * 8;
-constexpr int kGramBlocks = 148 * 2;
-
-// Shared row strides (doubles): roundup(M, 16) + 4 and 8 NT + 4 put the four rows of one fragment
-// load into distinct 32-byte bank groups.
-__host__ __device__ inline int gram_sq(int M) { return (M + 15) / 16 * 16 + 4; }
-
-// Partial A^T B over this block's rows -> part[blockIdx.x][a][c] (M x P, a-major).  Rows are
-// copied in 16-byte chunks when the pointer and stride allow it, else element by element.
-// Fragment layouts of m8n8k4 (row.col): A[m][k] sits in lane 4 m + k, B[k][n] in lane 4 n + k,
-// D[m][n] in lane 4 m + n / 2 (element n % 2).
+// Partial A^T B over this block's rows -> part[blockIdx.x][a][c] (Mc x P, a-major) for the
+// columns a0 .. a0 + Mc - 1 of A.  Warp w owns the tiles w, w + 16, ... of C.
 template <int NT>
-__global__ void __launch_bounds__(kThreads, 1) k_gram(const double* __restrict__ A, int lda,
+__global__ void __launch_bounds__(kGramThreads, 1) k_gram(const double* __restrict__ A, int lda,
                                                       const double* __restrict__ B, int ldb,
-                                                      int64_t n, int M, int P,
+                                                      int64_t n, int Mc, int P,
                                                       double* __restrict__ part) {
-  extern __shared__ double sm[];
-  const int SQ = gram_sq(M);
-  constexpr int SW = 8 * NT + 4;
-  double* sq = sm;
-  double* sw = sm + 2 * kGramRows * SQ;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
   const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(n, r0 + per);
-  const int mt_total = (M + 7) / 8;
-  double acc[kGramMT][NT][2];
+  const int mt_total = (Mc + 7) / 8;
+  double acc[kGramTiles][NT][2];
 #pragma unroll
-  for (int t = 0; t < kGramMT; ++t)
+  for (int t = 0; t < kGramTiles; ++t)
 #pragma unroll
     for (int u = 0; u < NT; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
-  const int qchunks = (M + 1) / 2, bchunks = (P + 1) / 2;
-  const bool va = ((lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
-  const bool vb = ((ldb & 1) == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
-  auto load = [&](int stage, int64_t i0) {
-    double* dq = sq + stage * kGramRows * SQ;
-    double* dw = sw + stage * kGramRows * SW;
-    for (int x = threadIdx.x; x < kGramRows * qchunks; x += kThreads) {
-      const int r = x / qchunks, c2 = x - r * qchunks;
-      const int64_t i = i0 + r;
-      double* d = dq + r * SQ + 2 * c2;
-      if (va && i < r1 && 2 * c2 + 1 < M) {
-        cp16(d, A + i * lda + 2 * c2);
-      } else {
-        d[0] = (i < r1 && 2 * c2 < M) ? A[i * lda + 2 * c2] : 0.0;
-        d[1] = (i < r1 && 2 * c2 + 1 < M) ? A[i * lda + 2 * c2 + 1] : 0.0;
-      }
-    }
-    for (int x = threadIdx.x; x < kGramRows * bchunks; x += kThreads) {
-      const int r = x / bchunks, c2 = x - r * bchunks;
-      const int64_t i = i0 + r;
-      double* d = dw + r * SW + 2 * c2;
-      if (vb && i < r1 && 2 * c2 + 1 < P) {
-        cp16(d, B + i * ldb + 2 * c2);
-      } else {
-        d[0] = (i < r1 && 2 * c2 < P) ? B[i * ldb + 2 * c2] : 0.0;
-        d[1] = (i < r1 && 2 * c2 + 1 < P) ? B[i * ldb + 2 * c2 + 1] : 0.0;
-      }
-    }
-    cp_commit();
-  };
-  const int64_t nst = r1 > r0 ? (r1 - r0 + kGramRows - 1) / kGramRows : 0;
-  if (nst > 0) load(0, r0);
-  for (int64_t s = 0; s < nst; ++s) {
-    if (s + 1 < nst) load((int)((s + 1) & 1), r0 + (s + 1) * kGramRows);
-    else cp_commit();
-    cp_wait1();
-    __syncthreads();
-    const double* dq = sq + (s & 1) * kGramRows * SQ;
-    const double* dw = sw + (s & 1) * kGramRows * SW;
+  int acol[kGramTiles];
+  bool aon[kGramTiles];
 #pragma unroll
-    for (int k = 0; k < kGramRows; k += 4) {
-      const int kr = k + (lane & 3);
-      double b[NT];
+  for (int t = 0; t < kGramTiles; ++t) {
+    acol[t] = 8 * (wid + kGramWarps * t) + (lane >> 2);
+    aon[t] = (wid + kGramWarps * t) < mt_total && acol[t] < Mc;
+  }
+  const int kl = lane & 3;
+  for (int64_t k0 = r0; k0 < r1; k0 += 4 * kGramUnroll) {
+    double a[kGramUnroll][kGramTiles], b[kGramUnroll][NT];
+#pragma unroll
+    for (int s = 0; s < kGramUnroll; ++s) {
+      const int64_t i = k0 + 4 * s + kl;
+      const bool rin = i < r1;
+#pragma unroll
+      for (int t = 0; t < kGramTiles; ++t)
+        a[s][t] = (rin && aon[t]) ? __ldg(A + i * lda + acol[t]) : 0.0;
 #pragma unroll
       for (int u = 0; u < NT; ++u) {
         const int c = 8 * u + (lane >> 2);
-        b[u] = c < P ? dw[kr * SW + c] : 0.0;
-      }
-#pragma unroll
-      for (int t = 0; t < kGramMT; ++t) {
-        const int mt = wid + 8 * t;
-        if (mt < mt_total) {
-          const int a = 8 * mt + (lane >> 2);
-          const double av = a < M ? dq[kr * SQ + a] : 0.0;
-#pragma unroll
-          for (int u = 0; u < NT; ++u) dmma(acc[t][u], av, b[u]);
-        }
+        b[s][u] = (rin && c < P) ? __ldg(B + i * ldb + c) : 0.0;
       }
     }
-    __syncthreads();
-  }
-  double* out = part + (int64_t)blockIdx.x * M * P;
 #pragma unroll
-  for (int t = 0; t < kGramMT; ++t) {
-    const int mt = wid + 8 * t;
+    for (int s = 0; s < kGramUnroll; ++s)
+#pragma unroll
+      for (int t = 0; t < kGramTiles; ++t)
+        if ((wid + kGramWarps * t) < mt_total)
+#pragma unroll
+          for (int u = 0; u < NT; ++u) dmma(acc[t][u], a[s][t], b[s][u]);
+  }
+  double* out = part + (int64_t)blockIdx.x * Mc * P;
+#pragma unroll
+  for (int t = 0; t < kGramTiles; ++t) {
+    const int mt = wid + kGramWarps * t;
     if (mt >= mt_total) continue;
-    const int a = 8 * mt + (lane >> 2);
-    if (a >= M) continue;
+    const int r = 8 * mt + (lane >> 2);
+    if (r >= Mc) continue;
 #pragma unroll
     for (int u = 0; u < NT; ++u)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int c = 8 * u + 2 * (lane & 3) + j;
-        if (c < P) out[(int64_t)a * P + c] = acc[t][u][j];
+        if (c < P) out[(int64_t)r * P + c] = acc[t][u][j];
       }
   }
 }
@@ -156,108 +118,104 @@ __global__ void k_gram_reduce(const double* __restrict__ part, int nblk, int M, 
   }
 }
 
-constexpr int kRowsTile = 64, kRowsKC = 32;
+// Shared row stride of the S slab: 8 NT + 4 doubles puts the four k-rows of one fragment load into
+// distinct 32-byte bank groups.
+constexpr int kRowsMaxM = 1280;     // rows of S held in shared memory per pass over A
 
 template <int NT>
-constexpr size_t rows_smem() {
-  return (size_t)(2 * kRowsTile * (kRowsKC + 4) + 2 * kRowsKC * (8 * NT + 4)) * sizeof(double);
+constexpr size_t rows_smem(int M) {
+  return (size_t)M * (8 * NT + 4) * sizeof(double);
 }
 
-// Out[i][c] = alpha sum_a A[i][a] S[a + c lds] + beta Out[i][c] for 64 rows and up to 8 NT
-// columns.  Shared memory: two stages of the A tile (64 x 36) and of the S tile (32 x 8 NT + 4).
+// Out[i][c] = alpha sum_a A[i][a] S[a + c lds] + beta Out[i][c] for the Mc rows of S starting
+// at a0 (accum: add this slab to Out, which already holds the earlier slabs' sum; the alpha/beta
+// update happens on the first slab).  Warps stream 8-row tiles of A over the whole grid.
 template <int NT>
-__global__ void __launch_bounds__(kThreads) k_rows(const double* __restrict__ A, int lda,
-                                                   const double* __restrict__ S, int lds,
-                                                   int64_t n, int M, int P, double alpha,
-                                                   double beta, double* __restrict__ Out,
-                                                   int ldo) {
-  extern __shared__ double smr[];
-  auto sa = reinterpret_cast<double(*)[kRowsTile][kRowsKC + 4]>(smr);
-  auto ss = reinterpret_cast<double(*)[kRowsKC][8 * NT + 4]>(smr + 2 * kRowsTile * (kRowsKC + 4));
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int64_t i0 = (int64_t)blockIdx.x * kRowsTile;
-  double acc[NT][2];
-#pragma unroll
-  for (int u = 0; u < NT; ++u) acc[u][0] = acc[u][1] = 0.0;
-  const int nk = (M + kRowsKC - 1) / kRowsKC;
-  const bool vec = ((lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
-  auto load = [&](int stage, int k0) {
-    for (int x = threadIdx.x; x < kRowsTile * (kRowsKC / 2); x += kThreads) {
-      const int r = x / (kRowsKC / 2), c2 = x - r * (kRowsKC / 2);
-      const int64_t i = i0 + r;
-      const int a = k0 + 2 * c2;
-      double* d = &sa[stage][r][2 * c2];
-      if (vec && i < n && a + 1 < M) {
-        cp16(d, A + i * lda + a);
-      } else {
-        d[0] = (i < n && a < M) ? A[i * lda + a] : 0.0;
-        d[1] = (i < n && a + 1 < M) ? A[i * lda + a + 1] : 0.0;
-      }
-    }
-    for (int x = threadIdx.x; x < kRowsKC * 8 * NT; x += kThreads) {
-      const int r = x / (8 * NT), c = x - r * (8 * NT);
-      const int a = k0 + r;
-      ss[stage][r][c] = (a < M && c < P) ? S[a + (int64_t)c * lds] : 0.0;
-    }
-    cp_commit();
-  };
-  load(0, 0);
-  for (int kc = 0; kc < nk; ++kc) {
-    if (kc + 1 < nk) load((kc + 1) & 1, (kc + 1) * kRowsKC);
-    else cp_commit();
-    cp_wait1();
-    __syncthreads();
-    const int st = kc & 1;
-#pragma unroll
-    for (int k = 0; k < kRowsKC; k += 4) {
-      const double av = sa[st][8 * wid + (lane >> 2)][k + (lane & 3)];
-#pragma unroll
-      for (int u = 0; u < NT; ++u) dmma(acc[u], av, ss[st][k + (lane & 3)][8 * u + (lane >> 2)]);
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(kThreads, 1) k_rows(const double* __restrict__ A, int lda,
+                                                      const double* __restrict__ S, int lds,
+                                                      int64_t n, int Mc, int P, double alpha,
+                                                      double beta, double* __restrict__ Out,
+                                                      int ldo) {
+  extern __shared__ double ss[];  // [Mc][8 NT + 4]
+  constexpr int SW = 8 * NT + 4;
+  for (int x = threadIdx.x; x < Mc * 8 * NT; x += blockDim.x) {
+    const int a = x / (8 * NT), c = x - a * (8 * NT);
+    ss[a * SW + c] = c < P ? S[a + (int64_t)c * lds] : 0.0;
   }
-  const int64_t i = i0 + 8 * wid + (lane >> 2);
-  if (i < n) {
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int kl = lane & 3;
+  const int64_t tiles = (n + 7) / 8;
+  const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile < tiles;
+       tile += wstride) {
+    const int64_t i = tile * 8 + (lane >> 2);
+    const bool rin = i < n;
+    const double* arow = A + (rin ? i : 0) * lda;
+    double acc[NT][2];
 #pragma unroll
-    for (int u = 0; u < NT; ++u)
+    for (int u = 0; u < NT; ++u) acc[u][0] = acc[u][1] = 0.0;
+    for (int k0 = 0; k0 < Mc; k0 += 4 * kUnroll) {
+      double a[kUnroll];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int c = 8 * u + 2 * (lane & 3) + j;
-        if (c < P) {
-          double* o = Out + i * ldo + c;
-          *o = beta == 0.0 ? alpha * acc[u][j] : alpha * acc[u][j] + beta * *o;
+      for (int s = 0; s < kUnroll; ++s) {
+        const int k = k0 + 4 * s + kl;
+        a[s] = (rin && k < Mc) ? __ldg(arow + k) : 0.0;
+      }
+#pragma unroll
+      for (int s = 0; s < kUnroll; ++s) {
+        const int k = k0 + 4 * s + kl;
+        if (k0 + 4 * s < Mc) {
+#pragma unroll
+          for (int u = 0; u < NT; ++u)
+            dmma(acc[u], a[s], k < Mc ? ss[k * SW + 8 * u + (lane >> 2)] : 0.0);
         }
       }
+    }
+    if (rin) {
+#pragma unroll
+      for (int u = 0; u < NT; ++u)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int c = 8 * u + 2 * (lane & 3) + j;
+          if (c < P) {
+            double* o = Out + i * ldo + c;
+            *o = beta == 0.0 ? alpha * acc[u][j] : alpha * acc[u][j] + beta * *o;
+          }
+        }
+    }
   }
+}
+
+// The dynamic shared-memory limits are set once per process to the largest size any launch uses,
+// so concurrent contexts never race on them.
+std::once_flag g_attr_once;
+void set_attributes() {
+  std::call_once(g_attr_once, [] {
+    cudaFuncSetAttribute(k_rows<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)rows_smem<1>(kRowsMaxM));
+    cudaFuncSetAttribute(k_rows<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)rows_smem<2>(kRowsMaxM));
+  });
 }
 
 }  // namespace
 
 int64_t proj_gram_scratch(int M, int P) {
-  return (int64_t)kGramBlocks * std::min(M, kGramSlab) * P;
+  return (int64_t)kBlocks * std::min(M, kGramSlab) * P;
 }
 
 bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, int M, int P,
                double alpha, double beta, double* C, int ldc, double* part, cudaStream_t s) {
   if (M <= 0 || P <= 0) return true;
   if (P > 16 || lda < M || ldb < P) return false;
-  const int NT = P <= 8 ? 1 : 2;
-  int nblk = kGramBlocks;
-  if (n < (int64_t)nblk * kGramRows)
-    nblk = (int)std::max<int64_t>(1, (n + kGramRows - 1) / kGramRows);
+  int nblk = kBlocks;
+  if (n < (int64_t)nblk * 64) nblk = (int)std::max<int64_t>(1, (n + 63) / 64);
   for (int a0 = 0; a0 < M; a0 += kGramSlab) {
     const int Mc = std::min(kGramSlab, M - a0);
-    const int SQ = gram_sq(Mc);
-    const size_t smem =
-        (size_t)(2 * kGramRows * SQ + 2 * kGramRows * (8 * NT + 4)) * sizeof(double);
     note_launch();
-    if (NT == 1) {
-      cudaFuncSetAttribute(k_gram<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_gram<1><<<nblk, kThreads, smem, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
-    } else {
-      cudaFuncSetAttribute(k_gram<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_gram<2><<<nblk, kThreads, smem, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
-    }
+    if (P <= 8) k_gram<1><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+    else k_gram<2><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
     note_launch();
     k_gram_reduce<<<(Mc * P + 255) / 256, 256, 0, s>>>(part, nblk, Mc, P, alpha, beta, C + a0,
                                                         ldc);
@@ -268,24 +226,25 @@ bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, in
 void proj_rows(const double* A, int lda, const double* S, int lds, int64_t n, int M, int P,
                double alpha, double beta, double* Out, int ldo, cudaStream_t s) {
   if (n <= 0 || P <= 0) return;
-  const unsigned g = (unsigned)((n + kRowsTile - 1) / kRowsTile);
-  for (int c0 = 0; c0 < P; c0 += 64) {
-    const int pc = std::min(64, P - c0);
-    const double* Sc = S + (int64_t)c0 * lds;
+  set_attributes();
+  const int64_t tiles = (n + 7) / 8;
+  const int g = (int)std::min<int64_t>(kBlocks, (tiles + 31) / 32);
+  for (int c0 = 0; c0 < P; c0 += 16) {
+    const int pc = std::min(16, P - c0);
     double* Oc = Out + c0;
-    note_launch();
-#define VHCI_ROWS(NTV)                                                                          \
-  do {                                                                                          \
-    cudaFuncSetAttribute(k_rows<NTV>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
-                         (int)rows_smem<NTV>());                                                \
-    k_rows<NTV><<<g, kThreads, rows_smem<NTV>(), s>>>(A, lda, Sc, lds, n, M, pc, alpha, beta,  \
-                                                      Oc, ldo);                                 \
-  } while (0)
-    if (pc <= 8) VHCI_ROWS(1);
-    else if (pc <= 16) VHCI_ROWS(2);
-    else if (pc <= 32) VHCI_ROWS(4);
-    else VHCI_ROWS(8);
-#undef VHCI_ROWS
+    // slabs of S rows; every slab after the first adds into Out
+    for (int a0 = 0; a0 < std::max(M, 1); a0 += kRowsMaxM) {
+      const int Mc = std::min(kRowsMaxM, M - a0);
+      const double* Sc = S + (int64_t)c0 * lds + a0;
+      const double bt = a0 == 0 ? beta : 1.0;
+      note_launch();
+      if (pc <= 8)
+        k_rows<1><<<g, kThreads, rows_smem<1>(std::max(Mc, 1)), s>>>(A + a0, lda, Sc, lds, n,
+                                                                     Mc, pc, alpha, bt, Oc, ldo);
+      else
+        k_rows<2><<<g, kThreads, rows_smem<2>(std::max(Mc, 1)), s>>>(A + a0, lda, Sc, lds, n,
+                                                                     Mc, pc, alpha, bt, Oc, ldo);
+    }
   }
 }
 

@@ -397,12 +397,7 @@ int block_lanczos(vhci_ctx* c, int k) {
   auto msince = [&](std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(now() - t0).count();
   };
-  int steps = 0, skipped = 0;
-  // VHCI_REORTH_KAPPA = K > 0: run the second Gram-Schmidt pass of a step only when some column's
-  // norm fell by more than a factor K in the first pass (the Daniel-Gragg-Kaufman-Stewart test
-  // with threshold K instead of sqrt(2)); 0 (default) runs it at every step
-  double kappa_max = 0.0;
-  if (const char* e = std::getenv("VHCI_REORTH_KAPPA")) kappa_max = std::atof(e);
+  int steps = 0;
   for (int cyc = 0; cyc < maxcyc; ++cyc) {
     // ---- expansion
     bool exhausted = (p == 0);
@@ -423,30 +418,8 @@ int block_lanczos(vhci_ctx* c, int k) {
       copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
       VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)std::max(m, b) * p, s));
-      bool second = true;
-      if (kappa_max > 0) {
-        // ||H q_c||^2 = ||T[:, c]||^2 + ||w_c||^2: the first pass removed the part of H q_c in
-        // span(Q); a classical pass leaves an orthogonality error of about eps * ||H q_c|| / ||w_c||
-        VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, nl, p, p, 1.0, 0.0, w.S.p, p));
-        std::vector<double> G((size_t)p * p), Tc((size_t)m * p);
-        VCK(d2h(c, G.data(), w.S.p, G.size() * sizeof(double)));
-        VCK(cudaMemcpy2DAsync(Tc.data(), m * sizeof(double), w.T.p + (size_t)(m - p) * ld,
-                              ld * sizeof(double), m * sizeof(double), p, cudaMemcpyDeviceToHost, s));
-        VCK(cudaStreamSynchronize(s));
-        double kmax = 0.0;
-        for (int cc = 0; cc < p; ++cc) {
-          double t2 = 0.0;
-          for (int a = 0; a < m; ++a) t2 += Tc[(size_t)cc * m + a] * Tc[(size_t)cc * m + a];
-          const double w2 = G[(size_t)cc * p + cc];
-          kmax = std::max(kmax, w2 > 0 ? std::sqrt((t2 + w2) / w2) : INFINITY);
-        }
-        second = kmax > kappa_max;
-        if (!second) ++skipped;
-      }
-      if (second) {
-        VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
-        VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
-      }
+      VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
       int p2 = 0;
       VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + m, ld, &p2));
       t_orth += msince(t0);
@@ -486,8 +459,8 @@ int block_lanczos(vhci_ctx* c, int k) {
       if (nconv < keff && !(m >= n || exhausted))
         return fail(c, VHCI_E_NOT_CONVERGED, "Error: Eigenvalues did not converge.");
       if (plevel)
-        std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d (second pass skipped %d) ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
-                     (long long)n, k, b, cyc + 1, steps, skipped, t_spmm, t_orth, t_rr, msince(t_start));
+        std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
+                     (long long)n, k, b, cyc + 1, steps, t_spmm, t_orth, t_rr, msince(t_start));
       VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
