@@ -107,7 +107,10 @@ typedef struct {
   int64_t h2d_bytes, d2h_bytes;   /* host<->device bytes copied by the library                 */
   int64_t kernel_launches;        /* this library's kernel launches so far (process-wide)      */
   int64_t spmm_gather_bytes;      /* vector-row bytes the sparse products gathered (nnz * b * 8
-                                     per product): the traffic that bounds them, mostly from L2 */
+                                     per product, 4 with FP32 gathers): the traffic that bounds
+                                     them, mostly from L2                                       */
+  double mixed_max_residual;      /* mixed precision: largest ||H x - theta x|| / max(1, |theta|)
+                                     of the Ritz pairs after the FP64 sweeps                     */
 } vhci_stats;
 
 typedef void (*vhci_iter_cb)(void* user, int iteration, int64_t n_basis, double zpe);

@@ -228,6 +228,67 @@ __global__ void __launch_bounds__(256) k_spmm_pairs(int64_t n, const int64_t* __
   }
 }
 
+// Mixed-precision form: the gathered vector block is FP32 (each lane owns four adjacent columns,
+// one 16-byte float4 gather), the matrix values FP32, the accumulation FP64, and the diagonal term
+// multiplies the FP64 block Xd (row i of the rows held, stride ldd).  A 16-column FP32 block row
+// is 64 bytes, half the gathered bytes of the FP64 form.
+template <int BQ>
+__global__ void __launch_bounds__(256) k_spmm_f32x(int64_t n, const int64_t* __restrict__ rowptr,
+                                                   const int32_t* __restrict__ col,
+                                                   const float* __restrict__ val,
+                                                   const double* __restrict__ diag,
+                                                   const float* __restrict__ X, int ldx, int bq,
+                                                   const double* __restrict__ Xd, int ldd,
+                                                   double* __restrict__ Y, int ldy) {
+  constexpr int G = 32 / BQ, U = 16;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / BQ, cc = lane % BQ;
+  const bool active = cc < bq;
+  const float4* __restrict__ X4 = reinterpret_cast<const float4*>(X);
+  const int ldx4 = ldx >> 2;
+  const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5) * G;
+  for (int64_t i = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * G + grp;
+       i < n; i += stride) {
+    if (!active) continue;
+    const int64_t beg = __ldg(rowptr + i), end = __ldg(rowptr + i + 1);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    auto acc = [&](double v, float4 x) {
+      a0 = fma(v, (double)x.x, a0);
+      a1 = fma(v, (double)x.y, a1);
+      a2 = fma(v, (double)x.z, a2);
+      a3 = fma(v, (double)x.w, a3);
+    };
+    auto gx = [&](int j) { return __ldg(X4 + (int64_t)j * ldx4 + cc); };
+    int64_t e = beg;
+    for (; e < end && (e & 3); ++e) acc((double)__ldg(val + e), gx(__ldg(col + e)));
+    for (; e + U <= end; e += U) {
+      int j[U];
+      float v[U];
+#pragma unroll
+      for (int u = 0; u < U; u += 4) {
+        const int4 jj = __ldg(reinterpret_cast<const int4*>(col + e + u));
+        j[u] = jj.x; j[u + 1] = jj.y; j[u + 2] = jj.z; j[u + 3] = jj.w;
+        const float4 vf = __ldg(reinterpret_cast<const float4*>(val + e + u));
+        v[u] = vf.x; v[u + 1] = vf.y; v[u + 2] = vf.z; v[u + 3] = vf.w;
+      }
+      float4 x[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) x[u] = gx(j[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) acc((double)v[u], x[u]);
+    }
+#pragma unroll 4
+    for (; e < end; ++e) acc((double)__ldg(val + e), gx(__ldg(col + e)));
+    const double d = diag[i];
+    const double* xd = Xd + i * ldd + 4 * cc;
+    double* y = Y + i * ldy + 4 * cc;
+    y[0] = fma(d, xd[0], a0);
+    y[1] = fma(d, xd[1], a1);
+    y[2] = fma(d, xd[2], a2);
+    y[3] = fma(d, xd[3], a3);
+  }
+}
+
 template <typename VT>
 void spmm_rows_launch(int64_t n, const int64_t* rowptr, const int32_t* col, const VT* val,
                       const double* diag, const double* X, int ldx, int b, double* Y, int ldy,
@@ -421,6 +482,42 @@ void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, con
     if (pvalf) spmm_rows_launch<float>(n, prow + (int64_t)p * n, pcol, pvalf, diag, X, ldx, b, Y, ldy, p > 0, xrow0, s);
     else spmm_rows_launch<double>(n, prow + (int64_t)p * n, pcol, pval, diag, X, ldx, b, Y, ldy, p > 0, xrow0, s);
   }
+}
+
+bool spmm_f32x(int64_t n, const int64_t* rowptr, const int32_t* col, const float* val,
+               const double* diag, const float* X, int ldx, int b, const double* Xd, int ldd,
+               double* Y, int ldy, cudaStream_t s) {
+  if (n <= 0 || b <= 0) return true;
+  if (b % 4 || ldx % 4 || reinterpret_cast<uintptr_t>(X) % 16) return false;
+  const int BQ = b <= 16 ? 4 : 8;  // lanes per row; 4 BQ columns per launch
+  const int gr = grid_for(n * BQ, 256, 148 * 16);
+  for (int c0 = 0; c0 < b; c0 += 4 * BQ) {
+    const int bq = std::min(BQ, (b - c0) / 4);
+    note_launch();
+    if (BQ == 8)
+      k_spmm_f32x<8><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bq, Xd + c0, ldd, Y + c0, ldy);
+    else
+      k_spmm_f32x<4><<<gr, 256, 0, s>>>(n, rowptr, col, val, diag, X + c0, ldx, bq, Xd + c0, ldd, Y + c0, ldy);
+  }
+  return true;
+}
+
+// Compact FP32 copy of ncol columns of a row-major FP64 block (rounded to nearest).
+__global__ void k_copy_cols_f32(const double* __restrict__ src, int lds, float* __restrict__ dst,
+                                int ldd, int64_t n, int ncol) {
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n * ncol;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / ncol;
+    const int c = (int)(idx % ncol);
+    dst[i * ldd + c] = (float)src[i * lds + c];
+  }
+}
+
+void copy_cols_f32(const double* src, int lds, float* dst, int ldd, int64_t n, int ncol,
+                   cudaStream_t s) {
+  if (n <= 0 || ncol <= 0) return;
+  note_launch();
+  k_copy_cols_f32<<<grid_for(n * ncol, 256), 256, 0, s>>>(src, lds, dst, ldd, n, ncol);
 }
 
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,

@@ -85,10 +85,13 @@ void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std::vecto
 
 struct LWork {
   DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc, gpart, Xg, gtmp;
+  DBuf<float> Xf, Xgf;  // FP32 copies of the vector block (mixed precision)
+  bool exact = false;   // mixed precision: products with FP64 gathers (the final sweep)
   void release(cudaStream_t s) {
     Q.release(s); HQ.release(s); T.release(s); Yw.release(s); theta.release(s); Xb.release(s);
     HXb.release(s); W.release(s); S.release(s); M.release(s); part.release(s); rn2.release(s);
-    Xc.release(s); gpart.release(s); Xg.release(s); gtmp.release(s);
+    Xc.release(s); gpart.release(s); Xg.release(s); gtmp.release(s); Xf.release(s);
+    Xgf.release(s);
   }
 };
 
@@ -209,17 +212,35 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
   VCK(ev_e0e1.create());
   cudaEvent_t e0 = ev_e0e1.a, e1 = ev_e0e1.b;
   const int64_t nl = c->nrow, rb = c->rblk;
-  VCK(w.Xc.reserve((size_t)std::max(nl, rb) * b, c->st));
   VCK(cudaEventRecord(e0, c->st));
-  copy_cols(X, ldx, w.Xc.p, b, nl, b, c->st);
-  const double* Xfull = w.Xc.p;
-  if (is_sharded(c)) {
-    if (nl < rb) fill_zero(w.Xc.p + (size_t)nl * b, (rb - nl) * (int64_t)b, c->st);
-    VCK(w.Xg.reserve((size_t)c->comm.nranks * rb * b, c->st));
-    VTRY(comm_gather(c, w.Xc.p, w.Xg.p, rb * b * (int64_t)sizeof(double)));
-    Xfull = w.Xg.p;
+  // mixed precision: FP32 block gathers, FP64 accumulation and diagonal term (needs 16-byte
+  // gathers of four columns; other widths, the final sweep and column panels gather FP64)
+  const bool f32x = c->o.precision == 1 && !w.exact && b % 4 == 0;
+  if (f32x) {
+    VCK(w.Xf.reserve((size_t)std::max(nl, rb) * b, c->st));
+    copy_cols_f32(X, ldx, w.Xf.p, b, nl, b, c->st);
+    const float* Xfull = w.Xf.p;
+    if (is_sharded(c)) {
+      if (nl < rb) VCK(cudaMemsetAsync(w.Xf.p + (size_t)nl * b, 0, (rb - nl) * b * sizeof(float), c->st));
+      VCK(w.Xgf.reserve((size_t)c->comm.nranks * rb * b, c->st));
+      VTRY(comm_gather(c, w.Xf.p, w.Xgf.p, rb * b * (int64_t)sizeof(float)));
+      Xfull = w.Xgf.p;
+    }
+    if (!spmm_f32x(nl, c->rowptr.p, c->col.p, c->valf.p, c->diag.p, Xfull, b, b, X, ldx, Y, ldy,
+                   c->st))
+      return fail(c, VHCI_E_STATE, "FP32 product with an unaligned block");
+  } else {
+    VCK(w.Xc.reserve((size_t)std::max(nl, rb) * b, c->st));
+    copy_cols(X, ldx, w.Xc.p, b, nl, b, c->st);
+    const double* Xfull = w.Xc.p;
+    if (is_sharded(c)) {
+      if (nl < rb) fill_zero(w.Xc.p + (size_t)nl * b, (rb - nl) * (int64_t)b, c->st);
+      VCK(w.Xg.reserve((size_t)c->comm.nranks * rb * b, c->st));
+      VTRY(comm_gather(c, w.Xc.p, w.Xg.p, rb * b * (int64_t)sizeof(double)));
+      Xfull = w.Xg.p;
+    }
+    spmm_h(c, Xfull, b, b, Y, ldy);
   }
-  spmm_h(c, Xfull, b, b, Y, ldy);
   VCK(cudaEventRecord(e1, c->st));
   VCK(cudaEventSynchronize(e1));
   VCK(cudaGetLastError());
@@ -229,8 +250,51 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
   c->stats.spmm_calls += 1;
   c->stats.spmm_cols += b;
   const int64_t sval = c->o.precision == 1 ? 4 : 8;
-  c->stats.spmm_gather_bytes += c->nnz * (int64_t)b * 8;
-  c->stats.spmm_bytes += c->nnz * (sval + 4) + (nl + 1) * 8 + nl * 8 + 2 * nl * (int64_t)b * 8;
+  const int64_t sx = f32x ? 4 : 8;
+  c->stats.spmm_gather_bytes += c->nnz * (int64_t)b * sx;
+  c->stats.spmm_bytes += c->nnz * (sval + 4) + (nl + 1) * 8 + nl * 8 + nl * (int64_t)b * (sx + 8);
+  return VHCI_OK;
+}
+
+// Mixed precision, after the FP32-gather eigensolve: one Rayleigh-Ritz over the nk Ritz vectors
+// held in w.Xb (rows held, ld kk) with FP64 products H V (FP32 values, FP64 gathers and
+// arithmetic), so the Ritz values and vectors carry no FP32 rounding of the vectors.  The rotated
+// vectors replace w.Xb, their products land in w.HXb (ld kk), their residual norms (squared) in
+// w.rn2 and their values in th.  Q and HQ (ld >= nk), no longer needed, are the work space.
+int fp64_sweep(vhci_ctx* c, LWork& w, int kk, int nk, int ld, std::vector<double>& th) {
+  const int64_t nl = c->nrow;
+  cudaStream_t s = c->st;
+  w.exact = true;
+  for (int j0 = 0; j0 < nk; j0 += 16) {
+    const int bw = std::min(16, nk - j0);
+    VTRY(apply_h_l(c, w, w.Xb.p + j0, kk, bw, w.HQ.p + j0, ld));
+  }
+  w.exact = false;
+  // T = V^T H V, column chunks of 16
+  for (int j0 = 0; j0 < nk; j0 += 16) {
+    const int bw = std::min(16, nk - j0);
+    VTRY(gemm_gram(c, w, w.Xb.p, kk, w.HQ.p + j0, ld, nl, nk, bw, 1.0, 0.0,
+                   w.T.p + (size_t)j0 * ld, ld));
+  }
+  VCK(cudaMemcpy2DAsync(w.Yw.p, ld * sizeof(double), w.T.p, ld * sizeof(double),
+                        nk * sizeof(double), nk, cudaMemcpyDeviceToDevice, s));
+  VTRY(syevd_l(c, w.Yw.p, nk, ld, w.theta.p));
+  VTRY(comm_bcast0(c, w.Yw.p, (int64_t)ld * nk));
+  VTRY(comm_bcast0(c, w.theta.p, nk));
+  VTRY(gemm_rows(c, w.Xb.p, kk, w.Yw.p, ld, nl, nk, nk, 1.0, 0.0, w.Q.p, ld));
+  VTRY(gemm_rows(c, w.HQ.p, ld, w.Yw.p, ld, nl, nk, nk, 1.0, 0.0, w.HXb.p, kk));
+  copy_cols(w.Q.p, ld, w.Xb.p, kk, nl, nk, s);
+  residual_norms(w.Xb.p, w.HXb.p, nl, kk, nk, w.theta.p, w.part.p, residual_blocks(nl), w.rn2.p, s);
+  VTRY(comm_sum(c, w.rn2.p, nk));
+  th.resize(nk);
+  VCK(d2h(c, th.data(), w.theta.p, nk * sizeof(double)));
+  std::vector<double> rn(nk);
+  VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
+  VCK(cudaStreamSynchronize(s));
+  double rmax = 0.0;
+  for (int j = 0; j < nk; ++j)
+    rmax = std::max(rmax, std::sqrt(std::max(rn[j], 0.0)) / std::max(1.0, std::fabs(th[j])));
+  c->stats.mixed_max_residual = std::max(c->stats.mixed_max_residual, rmax);
   return VHCI_OK;
 }
 
@@ -317,6 +381,9 @@ double lanczos_min_bytes(vhci_ctx* c, int k) {
 
 int block_lanczos_lean(vhci_ctx* c, int k);
 
+// Relative residual tolerance of the FP32-gather eigensolve in mixed precision.
+constexpr double kMixedTol = 1e-7;
+
 int block_lanczos(vhci_ctx* c, int k) {
   const int64_t n = c->n;
   // rows held by this rank (all n unless sharded)
@@ -336,7 +403,10 @@ int block_lanczos(vhci_ctx* c, int k) {
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
-  const double tol = c->o.eig_tol > 0 ? c->o.eig_tol : 1e-10;
+  // mixed precision: the FP32-gather products carry rounding noise of about 1e-8 of |theta|, so
+  // the Lanczos stops at 1e-7 and the final FP64 sweep corrects the Ritz pairs
+  const bool mixed = c->o.precision == 1;
+  const double tol = std::max(c->o.eig_tol > 0 ? c->o.eig_tol : 1e-10, mixed ? kMixedTol : 0.0);
   const double eps23 = std::pow(DBL_EPSILON, 2.0 / 3.0);
   const char* prof = std::getenv("VHCI_PROFILE");
   const int plevel = prof ? std::atoi(prof) : 0;
@@ -461,6 +531,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       if (plevel)
         std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
                      (long long)n, k, b, cyc + 1, steps, t_spmm, t_orth, t_rr, msince(t_start));
+      if (mixed) VTRY(fp64_sweep(c, w, kk, nk, ld, th));
       VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
@@ -487,6 +558,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       exhausted = true;
     }
     if (exhausted) {
+      if (mixed) VTRY(fp64_sweep(c, w, kk, nk, ld, th));
       VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
@@ -522,6 +594,7 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
   const int plevel = prof ? std::atoi(prof) : 0;
   const int64_t chunk = std::max<int64_t>(1024, (int64_t)(2.5e8 / (8.0 * kk)));
   LWork w;  // Q, T, Yw, theta, W (pending block), HQ (rows x b product), Xb (rotation chunk)
+  w.exact = true;  // no final sweep here: FP64 gathers throughout, also in mixed precision
   VCK(w.Q.reserve((size_t)nl * ld, s));
   VCK(w.HQ.reserve((size_t)nl * b, s));
   VCK(w.W.reserve((size_t)nl * b, s));

@@ -130,6 +130,14 @@ void spmm_panels(int64_t n, int P, const int64_t* prow, const int32_t* pcol, con
 void spmm(int64_t n, const int64_t* rowptr, const int32_t* col, const double* val,
           const float* valf, const double* diag, const double* X, int ldx, int b, double* Y,
           int ldy, int64_t xrow0, cudaStream_t s);
+// Mixed precision: FP32 values and FP32 gathered block X (16-byte aligned, b and ldx multiples of
+// 4), FP64 accumulation; the diagonal term multiplies the FP64 block Xd (row i of the rows held).
+// Returns false (nothing launched) when the shapes do not allow the 16-byte gathers.
+bool spmm_f32x(int64_t n, const int64_t* rowptr, const int32_t* col, const float* val,
+               const double* diag, const float* X, int ldx, int b, const double* Xd, int ldd,
+               double* Y, int ldy, cudaStream_t s);
+void copy_cols_f32(const double* src, int lds, float* dst, int ldd, int64_t n, int ncol,
+                   cudaStream_t s);
 // ---- eigensolver helpers ----
 // rn2[c] (c < kk) = sum_i (HX[i,c] - theta[c] X[i,c])^2   (block partials reduced on device)
 void residual_norms(const double* X, const double* HX, int64_t n, int ld, int kk,
