@@ -36,7 +36,7 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
 
 constexpr int kThreads = 1024;      // proj_rows: 32 warps, one block per SM
 constexpr int kBlocks = 148;
-constexpr int kUnroll = 4;          // proj_rows: k-steps of loads issued ahead
+constexpr int kUnroll = 8;          // proj_rows: k-steps of loads issued ahead
 constexpr int kGramThreads = 512;   // proj_gram: 16 warps with up to 128 registers each
 constexpr int kGramWarps = kGramThreads / 32;
 constexpr int kGramTiles = 6;       // 8-row tiles of C per warp: a slab of 16 x 6 x 8 = 768 rows
@@ -121,6 +121,7 @@ __global__ void k_gram_reduce(const double* __restrict__ part, int nblk, int M, 
 // Shared row stride of the S slab: 8 NT + 4 doubles puts the four k-rows of one fragment load into
 // distinct 32-byte bank groups.
 constexpr int kRowsMaxM = 1280;     // rows of S held in shared memory per pass over A
+constexpr int kRowsMaxM4 = 768;     // the same for 32-column slabs
 
 template <int NT>
 constexpr size_t rows_smem(int M) {
@@ -187,6 +188,129 @@ __global__ void __launch_bounds__(kThreads, 1) k_rows(const double* __restrict__
   }
 }
 
+// The second and third Gram-Schmidt passes over the same rows of A, fused:
+//   W <- W - A S1            (S1: M x P column-major)
+//   part[block] = A^T W      (with the updated W; this block's rows, M x P a-major)
+// A block walks chunks of 256 rows (32 warps x one 8-row tile): each warp updates its tile of W (A
+// from global memory, S1 from shared memory) and leaves the new rows in a shared copy; then every
+// warp adds A_chunk^T W_chunk to its 8-row tiles of the partial Gram product, re-reading the
+// chunk's rows of A, which the first phase has just brought into L2.  One pass over A from HBM
+// instead of two.
+constexpr int kFuseChunk = 256;
+constexpr int kFuseTiles = 3;       // Gram tiles per warp: M <= 32 x 3 x 8 = 768
+constexpr int kFuseMaxM = 32 * kFuseTiles * 8;
+
+template <int NT>
+constexpr size_t fuse_smem(int M) {
+  return (size_t)(M + kFuseChunk) * (8 * NT + 4) * sizeof(double);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kThreads, 1) k_rows_gram(const double* __restrict__ A, int lda,
+                                                           const double* __restrict__ S1, int lds,
+                                                           double* __restrict__ W, int ldw,
+                                                           int64_t n, int M, int P,
+                                                           double* __restrict__ part) {
+  extern __shared__ double smf[];
+  constexpr int SW = 8 * NT + 4;
+  double* sS = smf;               // [M][SW]
+  double* sW = smf + M * SW;      // [kFuseChunk][SW]
+  for (int x = threadIdx.x; x < M * 8 * NT; x += blockDim.x) {
+    const int a = x / (8 * NT), c = x - a * (8 * NT);
+    sS[a * SW + c] = c < P ? S1[a + (int64_t)c * lds] : 0.0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, kl = lane & 3;
+  const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
+  const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(n, r0 + per);
+  const int mt_total = (M + 7) / 8;
+  double g[kFuseTiles][NT][2];
+#pragma unroll
+  for (int t = 0; t < kFuseTiles; ++t)
+#pragma unroll
+    for (int u = 0; u < NT; ++u) g[t][u][0] = g[t][u][1] = 0.0;
+  for (int64_t c0 = r0; c0 < r1; c0 += kFuseChunk) {
+    // phase 1: this warp's 8 rows of W - A S1
+    const int64_t i = c0 + 8 * wid + (lane >> 2);
+    const bool rin = i < r1;
+    const double* arow = A + (rin ? i : 0) * lda;
+    double acc[NT][2];
+#pragma unroll
+    for (int u = 0; u < NT; ++u) acc[u][0] = acc[u][1] = 0.0;
+    for (int k0 = 0; k0 < M; k0 += 4 * kUnroll) {
+      double a[kUnroll];
+#pragma unroll
+      for (int s = 0; s < kUnroll; ++s) {
+        const int k = k0 + 4 * s + kl;
+        a[s] = (rin && k < M) ? __ldg(arow + k) : 0.0;
+      }
+#pragma unroll
+      for (int s = 0; s < kUnroll; ++s) {
+        const int k = k0 + 4 * s + kl;
+        if (k0 + 4 * s < M) {
+#pragma unroll
+          for (int u = 0; u < NT; ++u)
+            dmma(acc[u], a[s], k < M ? sS[k * SW + 8 * u + (lane >> 2)] : 0.0);
+        }
+      }
+    }
+    const int rl = 8 * wid + (lane >> 2);
+#pragma unroll
+    for (int u = 0; u < NT; ++u)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int c = 8 * u + 2 * (lane & 3) + j;
+        double wv = 0.0;
+        if (rin && c < P) {
+          wv = W[i * ldw + c] - acc[u][j];
+          W[i * ldw + c] = wv;
+        }
+        sW[rl * SW + c] = wv;
+      }
+    __syncthreads();
+    // phase 2: the partial Gram product of the chunk, this warp's tiles w, w + 32, w + 64
+    for (int kk = 0; kk < kFuseChunk; kk += 8) {
+      double a[2][kFuseTiles], b[2][NT];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int kr = kk + 4 * s + kl;
+        const int64_t ir = c0 + kr;
+        const bool in2 = ir < r1;
+#pragma unroll
+        for (int t = 0; t < kFuseTiles; ++t) {
+          const int col = 8 * (wid + 32 * t) + (lane >> 2);
+          a[s][t] = (in2 && col < M) ? __ldg(A + ir * lda + col) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < NT; ++u) b[s][u] = sW[kr * SW + 8 * u + (lane >> 2)];
+      }
+#pragma unroll
+      for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int t = 0; t < kFuseTiles; ++t)
+          if (wid + 32 * t < mt_total)
+#pragma unroll
+            for (int u = 0; u < NT; ++u) dmma(g[t][u], a[s][t], b[s][u]);
+    }
+    __syncthreads();
+  }
+  double* out = part + (int64_t)blockIdx.x * M * P;
+#pragma unroll
+  for (int t = 0; t < kFuseTiles; ++t) {
+    const int mt = wid + 32 * t;
+    if (mt >= mt_total) continue;
+    const int r = 8 * mt + (lane >> 2);
+    if (r >= M) continue;
+#pragma unroll
+    for (int u = 0; u < NT; ++u)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int c = 8 * u + 2 * (lane & 3) + j;
+        if (c < P) out[(int64_t)r * P + c] = g[t][u][j];
+      }
+  }
+}
+
 // The dynamic shared-memory limits are set once per process to the largest size any launch uses,
 // so concurrent contexts never race on them.
 std::once_flag g_attr_once;
@@ -196,6 +320,12 @@ void set_attributes() {
                          (int)rows_smem<1>(kRowsMaxM));
     cudaFuncSetAttribute(k_rows<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)rows_smem<2>(kRowsMaxM));
+    cudaFuncSetAttribute(k_rows<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)rows_smem<4>(kRowsMaxM4));
+    cudaFuncSetAttribute(k_rows_gram<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)fuse_smem<1>(kFuseMaxM));
+    cudaFuncSetAttribute(k_rows_gram<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)fuse_smem<2>(kFuseMaxM));
   });
 }
 
@@ -223,14 +353,34 @@ bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, in
   return true;
 }
 
+bool proj_rows_gram(const double* A, int lda, const double* S1, int lds, double* W, int ldw,
+                    int64_t n, int M, int P, double* C, int ldc, double* part, cudaStream_t s) {
+  if (M <= 0 || P <= 0 || n <= 0) return true;
+  if (M > kFuseMaxM || P > 16 || lda < M || ldw < P) return false;
+  set_attributes();
+  int nblk = kBlocks;
+  if (n < (int64_t)nblk * kFuseChunk)
+    nblk = (int)std::max<int64_t>(1, (n + kFuseChunk - 1) / kFuseChunk);
+  note_launch();
+  if (P <= 8)
+    k_rows_gram<1><<<nblk, kThreads, fuse_smem<1>(M), s>>>(A, lda, S1, lds, W, ldw, n, M, P, part);
+  else
+    k_rows_gram<2><<<nblk, kThreads, fuse_smem<2>(M), s>>>(A, lda, S1, lds, W, ldw, n, M, P, part);
+  note_launch();
+  k_gram_reduce<<<(M * P + 255) / 256, 256, 0, s>>>(part, nblk, M, P, 1.0, 0.0, C, ldc);
+  return true;
+}
+
 void proj_rows(const double* A, int lda, const double* S, int lds, int64_t n, int M, int P,
                double alpha, double beta, double* Out, int ldo, cudaStream_t s) {
   if (n <= 0 || P <= 0) return;
   set_attributes();
   const int64_t tiles = (n + 7) / 8;
   const int g = (int)std::min<int64_t>(kBlocks, (tiles + 31) / 32);
-  for (int c0 = 0; c0 < P; c0 += 16) {
-    const int pc = std::min(16, P - c0);
+  // 32-column slabs when S's rows fit beside them in shared memory: half the passes over A
+  const int cw = (P > 16 && M <= kRowsMaxM4) ? 32 : 16;
+  for (int c0 = 0; c0 < P; c0 += cw) {
+    const int pc = std::min(cw, P - c0);
     double* Oc = Out + c0;
     // slabs of S rows; every slab after the first adds into Out
     for (int a0 = 0; a0 < std::max(M, 1); a0 += kRowsMaxM) {
@@ -238,7 +388,10 @@ void proj_rows(const double* A, int lda, const double* S, int lds, int64_t n, in
       const double* Sc = S + (int64_t)c0 * lds + a0;
       const double bt = a0 == 0 ? beta : 1.0;
       note_launch();
-      if (pc <= 8)
+      if (pc > 16)
+        k_rows<4><<<g, kThreads, rows_smem<4>(std::max(Mc, 1)), s>>>(A + a0, lda, Sc, lds, n,
+                                                                     Mc, pc, alpha, bt, Oc, ldo);
+      else if (pc <= 8)
         k_rows<1><<<g, kThreads, rows_smem<1>(std::max(Mc, 1)), s>>>(A + a0, lda, Sc, lds, n,
                                                                      Mc, pc, alpha, bt, Oc, ldo);
       else

@@ -149,6 +149,33 @@ int gemm_rows(vhci_ctx* c, const double* A, int lda, const double* S, int lds, i
   return VHCI_OK;
 }
 
+// The second and third Gram-Schmidt passes: W <- W - Q S1, then C = Q^T W (M x P, column-major),
+// fused into one pass over Q's rows when the shapes allow (k_proj.cu), else as two products.
+int gemm_rows_gram(vhci_ctx* c, LWork& w, const double* Q, int ldq, const double* S1, int lds,
+                   int64_t n, int M, int P, double* W, int ldw, double* C, int ldc) {
+  if (!proj_blas()) {
+    const bool sh = is_sharded(c);
+    double* out = C;
+    int ldo = ldc;
+    if (sh) {
+      VCK(w.gtmp.reserve((size_t)M * P, c->st));
+      out = w.gtmp.p;
+      ldo = M;
+    }
+    VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
+    if (proj_rows_gram(Q, ldq, S1, lds, W, ldw, n, M, P, out, ldo, w.gpart.p, c->st)) {
+      if (sh) {
+        VTRY(comm_sum(c, out, (int64_t)M * P));
+        VCK(cudaMemcpy2DAsync(C, ldc * sizeof(double), out, M * sizeof(double),
+                              M * sizeof(double), P, cudaMemcpyDeviceToDevice, c->st));
+      }
+      return VHCI_OK;
+    }
+  }
+  VTRY(gemm_rows(c, Q, ldq, S1, lds, n, M, P, -1.0, 1.0, W, ldw));
+  return gemm_gram(c, w, Q, ldq, W, ldw, n, M, P, 1.0, 0.0, C, ldc);
+}
+
 int syevd_l(vhci_ctx* c, double* A, int m, int lda, double* w) {
   int lwork = 0;
   VBL(cusolverDnDsyevd_bufferSize(c->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m, A,
@@ -486,9 +513,9 @@ int block_lanczos(vhci_ctx* c, int k) {
       }
       // next block: W = H Q_new - Q T[:, new]; second Gram-Schmidt pass; SVQB
       copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
-      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)std::max(m, b) * p, s));
-      VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+      VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, w.W.p, b,
+                          w.S.p, m));
       VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
       int p2 = 0;
       VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + m, ld, &p2));
@@ -539,9 +566,9 @@ int block_lanczos(vhci_ctx* c, int k) {
     // ---- thick restart: pending block from the last expansion, then keep the Ritz block
     t0 = now();
     copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
-    VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
     VCK(w.S.reserve((size_t)m * p, s));
-    VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+    VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, w.W.p, b,
+                        w.S.p, m));
     VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
     copy_cols(w.Xb.p, kk, w.Q.p, ld, nl, nk, s);
     copy_cols(w.HXb.p, kk, w.HQ.p, ld, nl, nk, s);
@@ -681,9 +708,9 @@ int block_lanczos_lean(vhci_ctx* c, int k) {
       plast = p;
       // pending block W = H Q_new - Q T[:, new], second Gram-Schmidt pass
       VCK(cudaMemcpyAsync(w.W.p, w.HQ.p, (size_t)nl * b * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      VTRY(gemm_rows(c, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, -1.0, 1.0, w.W.p, b));
       VCK(w.S.reserve((size_t)m * p, s));
-      VTRY(gemm_gram(c, w, w.Q.p, ld, w.W.p, b, nl, m, p, 1.0, 0.0, w.S.p, m));
+      VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, w.W.p, b,
+                          w.S.p, m));
       VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
       if (m + b > mmax || m >= n) break;
       int p2 = 0;

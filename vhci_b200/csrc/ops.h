@@ -160,6 +160,10 @@ bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, in
 // column-major (lds); any P (column chunks of 64).
 void proj_rows(const double* A, int lda, const double* S, int lds, int64_t n, int M, int P,
                double alpha, double beta, double* Out, int ldo, cudaStream_t s);
+// W <- W - A S1, then C (M x P, column-major) = A^T W, in one pass over A; M <= 768, P <= 16
+// (false, nothing launched, otherwise); part holds proj_gram_scratch(M, P) doubles.
+bool proj_rows_gram(const double* A, int lda, const double* S1, int lds, double* W, int ldw,
+                    int64_t n, int M, int P, double* C, int ldc, double* part, cudaStream_t s);
 
 // ---- PT2 (k_pt2.cu) ----
 void pt2_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
