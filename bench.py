@@ -57,6 +57,8 @@ L2_NOTE = "working set larger than L2 (Hamiltonian of 0.2-3 GB), no flush needed
 def bench_config(workload: int, batch: int) -> dict:
     """The `config` object both arms print: the workload and the solves per step."""
     return {"workload": WORKLOAD_DESCS[workload], "global_batch": batch, "l2": L2_NOTE}
+
+
 # Basis size after each heat-bath iteration and |P| of the workload-1 solve (FP64 path).
 WORKLOAD_COUNTS = {"sizes": [38934, 215006, 336950, 372333, 380418], "n_pert": 6583465}
 # DRAM bytes per k_spmm_rows launch, averaged over the 1085 launches of one workload-1 solve, from
