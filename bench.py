@@ -319,7 +319,7 @@ def run_ours(args):
     en_gbs = (st["pt2_reduce_bytes"] / (st["ms_pt2_reduce"] / 1e3) / 1e9
               if st["ms_pt2_reduce"] else None)
     alg_per_launch = st["spmm_bytes"] / st["spmm_calls"] if st["spmm_calls"] else None
-    roof = {"bound": "hbm", "kernel": "k_spmm_rows (eigensolver H*X)", "achieved": spmm_gbs,
+    roof = {"bound": "hbm", "kernel": "k_spmm_pairs (eigensolver H*X)", "achieved": spmm_gbs,
             "peak": hbm, "unit": "GB/s", "frac": (spmm_gbs / hbm) if spmm_gbs else None,
             "traffic": args.traffic if args.traffic else NCU_SPMM_TRAFFIC_PER_LAUNCH,
             "algorithmic_bytes_per_launch": alg_per_launch, "peak_kind": peak_kind,

@@ -9,6 +9,11 @@ the perturb-0 file, then PT2 runs on the same vectors and the corrected levels a
 the perturb-1 file, level by level in the reference's output order (E_0, then E_n - E_0; PT2
 output is not re-sorted, VHCI.cpp:118).
 
+The published naphthalene files list two pairs of excited levels out of ascending order (lines 13/14
+and 21/22 of the ε1 = 1.5 file, 21/22 of the ε1 = 1 file); this build reproduces their ZPE to
+1e-10 cm^-1, their basis growth, and every level to 2e-9 cm^-1 as a sorted list.  So excited levels
+are compared as sorted lists, the ZPE (line 0) on its own.
+
 Naphthalene has 48 modes, so its keys span three 64-bit words: this is the real-PES counterpart
 of the 48-mode benchmark shape.  Bars: 1e-4 cm^-1 for variational levels, 1e-3 cm^-1 after PT2,
 as for the other fixtures.  A published file that a current run of the reference does not
@@ -52,6 +57,12 @@ def _published_levels(name):
     return np.array([float(r.split()[0]) for r in rows if r.strip()])
 
 
+def _level_error(lev, ref):
+    """Largest difference: the ZPE, then the excited levels as sorted lists."""
+    lev = np.asarray(lev[:len(ref)])
+    return max(abs(lev[0] - ref[0]), float(np.abs(np.sort(lev[1:]) - np.sort(ref[1:])).max()))
+
+
 def write_input(path, mol, eps1, nstate, pt2, eps2, ntot):
     lines = open(os.path.join(PUB, mol + ".inp")).read().splitlines()
     for i, v in ((1, eps1), (2, nstate), (3, pt2), (4, eps2), (5, ntot)):
@@ -77,11 +88,11 @@ def test_published_levels(key, tmp_path):
         if g["var"]:
             ref = _published_levels(g["var"])
             assert len(ref) == min(nstate, v.n)
-            err = np.abs(lev_var[:len(ref)] - ref).max()
+            err = _level_error(lev_var, ref)
             assert err <= E_TOL, (g["var"], err)
         if g["pt2"]:
             v.pt2(eps2)
             lev = levels_of(v.energies()[:nstate])
             ref = _published_levels(g["pt2"][0])
-            err = np.abs(lev[:len(ref)] - ref).max()
+            err = _level_error(lev, ref)
             assert err <= PT2_TOL, (g["pt2"][0], err)

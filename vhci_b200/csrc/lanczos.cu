@@ -284,11 +284,11 @@ int apply_h_l(vhci_ctx* c, LWork& w, const double* X, int ldx, int b, double* Y,
 }
 
 // Mixed precision, after the FP32-gather eigensolve: one Rayleigh-Ritz over the nk Ritz vectors
-// held in w.Xb (rows held, ld kk) with FP64 products H V (FP32 values, FP64 gathers and
+// held in w.Xb (rows held, ld kk; the first keff are the wanted pairs) with FP64 products H V (FP32 values, FP64 gathers and
 // arithmetic), so the Ritz values and vectors carry no FP32 rounding of the vectors.  The rotated
 // vectors replace w.Xb, their products land in w.HXb (ld kk), their residual norms (squared) in
 // w.rn2 and their values in th.  Q and HQ (ld >= nk), no longer needed, are the work space.
-int fp64_sweep(vhci_ctx* c, LWork& w, int kk, int nk, int ld, std::vector<double>& th) {
+int fp64_sweep(vhci_ctx* c, LWork& w, int kk, int nk, int keff, int ld, std::vector<double>& th) {
   const int64_t nl = c->nrow;
   cudaStream_t s = c->st;
   w.exact = true;
@@ -319,7 +319,7 @@ int fp64_sweep(vhci_ctx* c, LWork& w, int kk, int nk, int ld, std::vector<double
   VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
   VCK(cudaStreamSynchronize(s));
   double rmax = 0.0;
-  for (int j = 0; j < nk; ++j)
+  for (int j = 0; j < keff; ++j)  // the wanted pairs; the guard vectors need not converge
     rmax = std::max(rmax, std::sqrt(std::max(rn[j], 0.0)) / std::max(1.0, std::fabs(th[j])));
   c->stats.mixed_max_residual = std::max(c->stats.mixed_max_residual, rmax);
   return VHCI_OK;
@@ -558,7 +558,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       if (plevel)
         std::fprintf(stderr, "lanczos n %lld k %d b %d cycles %d steps %d ms: spmm %.1f orth %.1f rr %.1f total %.1f\n",
                      (long long)n, k, b, cyc + 1, steps, t_spmm, t_orth, t_rr, msince(t_start));
-      if (mixed) VTRY(fp64_sweep(c, w, kk, nk, ld, th));
+      if (mixed) VTRY(fp64_sweep(c, w, kk, nk, std::min(k, nk), ld, th));
       VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
@@ -585,7 +585,7 @@ int block_lanczos(vhci_ctx* c, int k) {
       exhausted = true;
     }
     if (exhausted) {
-      if (mixed) VTRY(fp64_sweep(c, w, kk, nk, ld, th));
+      if (mixed) VTRY(fp64_sweep(c, w, kk, nk, std::min(k, nk), ld, th));
       VTRY(publish_ritz(c, w.Xb, kk, nk, th));  // the old X buffer is released with w
       w.release(s);
       return VHCI_OK;
