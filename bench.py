@@ -369,30 +369,45 @@ def run_ours(args):
 
 
 def run_spmm_sweep(args):
-    """Solve the workload, then time the sparse product H X on the final basis for several block
-    widths and both panel kernels (CUDA events around the product only)."""
+    """Time the sparse product H X on the workload's final variational basis for block widths
+    4-32 (CUDA events around the product only), then one eigensolve of the Nstate lowest pairs on
+    that basis.  With --checkpoint PATH the basis is read from PATH when the file exists, so that
+    nothing but the H build runs before the timed products (a profiler capture of them then starts
+    after a handful of launches and holds only H and the blocks on the device); otherwise the
+    workload is solved variationally and its basis written to PATH."""
     import numpy as np
     from vhci_b200 import api
     td = tempfile.mkdtemp(prefix="vhci_sweep_")
     path = os.path.join(td, "workload.inp")
-    write_workload(path)
+    write_workload(path, args.workload)
     with api.VHCI(path) as v:
-        v.hci()
+        if args.checkpoint and os.path.exists(args.checkpoint):
+            v.read_checkpoint(args.checkpoint)
+        else:
+            v.hci()
+            if args.checkpoint:
+                v.write_checkpoint(args.checkpoint)
+        nnz = v.build_h()
         rng = np.random.default_rng(0)
-        print(json.dumps({"n": v.n, "nnz": int(v.info.h_nnz)}), flush=True)
+        print(json.dumps({"n": v.n, "nnz": int(nnz)}), flush=True)
         for b in (4, 8, 16, 32):
             X = rng.standard_normal((v.n, b))
-            for form in ("rows", "slots"):
-                os.environ["VHCI_SPMM"] = form
+            v.apply_h(X)
+            s0 = v.stats()
+            for _ in range(args.sweep_reps):
                 v.apply_h(X)
-                s0 = v.stats()
-                for _ in range(8):
-                    v.apply_h(X)
-                s1 = v.stats()
-                ms = (s1["ms_spmm"] - s0["ms_spmm"]) / 8
-                print(json.dumps({"b": b, "kernel": form, "ms": round(ms, 3),
-                                  "ms_per_column": round(ms / b, 4)}), flush=True)
-        os.environ.pop("VHCI_SPMM", None)
+            s1 = v.stats()
+            ms = (s1["ms_spmm"] - s0["ms_spmm"]) / args.sweep_reps
+            gbs = (s1["spmm_bytes"] - s0["spmm_bytes"]) / args.sweep_reps / (ms / 1e3) / 1e9
+            print(json.dumps({"b": b, "ms": round(ms, 3), "ms_per_column": round(ms / b, 4),
+                              "algorithmic_GBs": round(gbs, 1)}), flush=True)
+        if args.sweep_eigs:
+            k = min(int(v.info.nstate), v.n)
+            s0 = v.stats()
+            v.eigs(k)
+            s1 = v.stats()
+            print(json.dumps({"eigs_k": k, "ms_eigs": round(s1["ms_eigs"] - s0["ms_eigs"], 1),
+                              "ms_spmm": round(s1["ms_spmm"] - s0["ms_spmm"], 1)}), flush=True)
 
 
 def _write_serving_request(r, path):
@@ -532,6 +547,11 @@ def main():
                     help="ncu dram bytes per SpMM launch, if captured")
     ap.add_argument("--spmm-sweep", action="store_true",
                     help="time the sparse product on the workload's final basis and exit")
+    ap.add_argument("--checkpoint", default=None,
+                    help="with --spmm-sweep: basis file read if present, written otherwise")
+    ap.add_argument("--sweep-reps", type=int, default=8)
+    ap.add_argument("--sweep-eigs", action="store_true",
+                    help="with --spmm-sweep: also time one eigensolve on the basis")
     ap.add_argument("--serving", action="store_true",
                     help="run the request-serving stream (one GPU) and exit")
     ap.add_argument("--requests", type=int, default=64)
