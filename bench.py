@@ -506,25 +506,36 @@ def run_serving(args):
 
 
 def run_mixed_check(args):
-    """Mixed precision (FP32 Hamiltonian values, FP64 accumulation, FP64 orthogonalisation, Ritz
-    values and PT2 denominators) against the FP64 path on one workload: device time of each (second
-    of two solves), basis and perturber counts, and the per-state error of the variational and
-    PT2-corrected energies."""
+    """Mixed precision (FP32 Hamiltonian values and FP32 vector gathers in the eigensolver's
+    products, FP64 accumulation, orthogonalisation, Ritz values, final Rayleigh-Ritz sweep and PT2)
+    against the FP64 path on one workload: device time of each (median of --mixed-reps alternating
+    solves after one warm-up pair) with its phases, basis and perturber counts, and the per-state
+    error of the variational and PT2-corrected energies."""
     import numpy as np
     from vhci_b200 import api, pes
     td = tempfile.mkdtemp(prefix="vhci_mixed_")
     path = os.path.join(td, "workload.inp")
     pes.write_workload(path, args.workload)
-    res = {}
-    for prec in (0, 1, 0, 1):
-        r = api.solve(path, precision=prec)
-        s = r["stats"]
-        res[prec] = (r, (s["ms_total"] + s["ms_pt2"]) / 1e3)
-    (a, ta), (b, tb) = res[0], res[1]
+    res, times, phases = {}, {0: [], 1: []}, {0: [], 1: []}
+    keys = ("ms_select", "ms_hbuild", "ms_eigs", "ms_spmm", "ms_pt2")
+    for rep in range(args.mixed_reps + 1):
+        for prec in (0, 1):
+            r = api.solve(path, precision=prec)
+            s = r["stats"]
+            res[prec] = r
+            if rep > 0:     # the first pair warms up
+                times[prec].append((s["ms_total"] + s["ms_pt2"]) / 1e3)
+                phases[prec].append([s[q] for q in keys])
+    a, b = res[0], res[1]
+    ta, tb = statistics.median(times[0]), statistics.median(times[1])
     k = min(len(a["E"]), len(b["E"]))
     line = {
         "metric": "mixed_vs_fp64", "workload": args.workload,
         "fp64_s": round(ta, 3), "mixed_s": round(tb, 3), "speedup": round(ta / tb, 3),
+        "solves_each": args.mixed_reps, "fp64_s_all": [round(t, 3) for t in times[0]],
+        "mixed_s_all": [round(t, 3) for t in times[1]],
+        "phase_ms_median": {q: [round(statistics.median(p[i] for p in phases[prec]), 1)
+                                for prec in (0, 1)] for i, q in enumerate(keys)},
         "n_basis": [a["n_basis"], b["n_basis"]], "n_pert": [a["n_pert"], b["n_pert"]],
         "max_abs_dE_variational_cm1": float(np.abs(a["E_var"][:k] - b["E_var"][:k]).max()),
         "max_abs_dE_cm1": float(np.abs(a["E"][:k] - b["E"][:k]).max()),
@@ -562,6 +573,7 @@ def main():
     ap.add_argument("--verbose-requests", action="store_true")
     ap.add_argument("--mixed-check", action="store_true",
                     help="solve a workload in FP64 and in mixed precision, report per-state errors")
+    ap.add_argument("--mixed-reps", type=int, default=3)
     ap.add_argument("--workload", type=int, default=WORKLOAD)
     args = ap.parse_args()
     if args.spmm_sweep:
