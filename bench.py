@@ -61,10 +61,13 @@ def bench_config(workload: int, batch: int) -> dict:
 
 # Basis size after each heat-bath iteration and |P| of the workload-1 solve (FP64 path).
 WORKLOAD_COUNTS = {"sizes": [38934, 215006, 336950, 372333, 380418], "n_pert": 6583465}
-# DRAM bytes per k_spmm_rows launch, averaged over the 1085 launches of one workload-1 solve, from
-# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of
-# `vhci_b200/bin/vhci -n 1 -i <workload-1 input> -o <out>` on B200.
-NCU_SPMM_TRAFFIC_PER_LAUNCH = 2.839e9
+# DRAM traffic of one k_spmm_pairs launch over its algorithmic bytes, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum = 4.186e9 + 0.051e9 bytes) of a 16-column product
+# on the final workload-1 basis (380,418 rows, 255,052,558 entries; algorithmic 3.164e9 bytes) by
+# `python bench.py --spmm-sweep --sweep-eigs --sweep-reps 2 --checkpoint <file>` on B200.  The
+# bench's launches run on every basis of the solve, so their traffic is this ratio times their
+# algorithmic bytes (the excess is vector-block gathers that miss L2, which scales with the entries).
+NCU_SPMM_TRAFFIC_RATIO = (4.186275e9 + 0.051259e9) / 3.1641044e9
 
 
 def _dist():
@@ -321,7 +324,10 @@ def run_ours(args):
     alg_per_launch = st["spmm_bytes"] / st["spmm_calls"] if st["spmm_calls"] else None
     roof = {"bound": "hbm", "kernel": "k_spmm_pairs (eigensolver H*X)", "achieved": spmm_gbs,
             "peak": hbm, "unit": "GB/s", "frac": (spmm_gbs / hbm) if spmm_gbs else None,
-            "traffic": args.traffic if args.traffic else NCU_SPMM_TRAFFIC_PER_LAUNCH,
+            "traffic": (args.traffic if args.traffic else
+                        NCU_SPMM_TRAFFIC_RATIO * alg_per_launch if alg_per_launch else None),
+            "traffic_note": ("ncu DRAM bytes of a captured final-basis launch, scaled to the "
+                             "average launch by algorithmic bytes"),
             "algorithmic_bytes_per_launch": alg_per_launch, "peak_kind": peak_kind,
             "other": {"k_pt2_en GB/s": en_gbs,
                       # the product's bound: each of the nnz entries gathers one b-column vector

@@ -153,11 +153,14 @@ __global__ void __launch_bounds__(256) k_spmm_rows(int64_t n, const int64_t* __r
 
 // Column-pair form of the row-group SpMM: each lane owns two adjacent columns and gathers them as
 // one 16-byte load, so a 16-column block row (128 bytes) takes 8 lanes and a warp holds 4 rows;
-// sixteen entries per iteration keep sixteen 16-byte gathers in flight per lane.  Measured on the
-// 380k-state workload-1 matrix (b = 16): 2.99 ms against 3.35 ms for one column per lane.  Needs X
-// and Y 16-byte aligned with even strides (the launcher checks).
+// sixteen entries per iteration keep sixteen 16-byte gathers in flight per lane.  The product is
+// bound by the latency of those gathers (L2 at under half its throughput), so the register budget
+// is set for four resident blocks per SM (64 registers): the compiler then keeps all sixteen
+// gathers in flight, where at its own choice (40 registers, six blocks) it kept fewer.  Measured on
+// the 380k-state workload-1 matrix (b = 16): 2.62 ms, against 2.96 ms at 40 registers and 3.35 ms
+// for one column per lane.  Needs X and Y 16-byte aligned with even strides (the launcher checks).
 template <int BQ, typename VT>
-__global__ void __launch_bounds__(256) k_spmm_pairs(int64_t n, const int64_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(256, 4) k_spmm_pairs(int64_t n, const int64_t* __restrict__ rowptr,
                                                     const int32_t* __restrict__ col,
                                                     const VT* __restrict__ val,
                                                     const double* __restrict__ diag,
@@ -231,9 +234,9 @@ __global__ void __launch_bounds__(256) k_spmm_pairs(int64_t n, const int64_t* __
 // Mixed-precision form: the gathered vector block is FP32 (each lane owns four adjacent columns,
 // one 16-byte float4 gather), the matrix values FP32, the accumulation FP64, and the diagonal term
 // multiplies the FP64 block Xd (row i of the rows held, stride ldd).  A 16-column FP32 block row
-// is 64 bytes, half the gathered bytes of the FP64 form.
+// is 64 bytes, half the gathered bytes of the FP64 form.  Register budget as for k_spmm_pairs.
 template <int BQ>
-__global__ void __launch_bounds__(256) k_spmm_f32x(int64_t n, const int64_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(256, 4) k_spmm_f32x(int64_t n, const int64_t* __restrict__ rowptr,
                                                    const int32_t* __restrict__ col,
                                                    const float* __restrict__ val,
                                                    const double* __restrict__ diag,

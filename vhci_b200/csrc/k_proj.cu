@@ -43,38 +43,47 @@ constexpr int kGramTiles = 6;       // 8-row tiles of C per warp: a slab of 16 x
 constexpr int kGramSlab = kGramWarps * kGramTiles * 8;
 constexpr int kGramUnroll = 2;
 
-// Partial A^T B over this block's rows -> part[blockIdx.x][a][c] (Mc x P, a-major) for the
-// columns a0 .. a0 + Mc - 1 of A.  Warp w owns the tiles w, w + 16, ... of C.
-template <int NT>
+// Partial A^T B over this block's rows for the columns a0 .. a0 + Mc - 1 of A.  The 8-row tiles
+// of C are dealt to a group of WG = ceil(tiles / TILES) warps (warp g of a group owns tiles g,
+// g + WG, ...); the block's 16 warps form 16 / WG such groups, which take turns over the block's
+// rows in steps of 4 UNROLL rows, so a narrow C (few tiles) still keeps every warp streaming.
+// When a group would need more than half the warps, all 16 form one group.
+// Group r of block x writes its partial to part[x * groups + r] (Mc x P, a-major).
+template <int NT, int TILES, int UNROLL>
 __global__ void __launch_bounds__(kGramThreads, 1) k_gram(const double* __restrict__ A, int lda,
                                                       const double* __restrict__ B, int ldb,
                                                       int64_t n, int Mc, int P,
                                                       double* __restrict__ part) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int mt_total = (Mc + 7) / 8;
+  int WG = (mt_total + TILES - 1) / TILES;
+  if (2 * WG > kGramWarps) WG = kGramWarps;  // one group: spread the tiles over all warps
+  const int RG = kGramWarps / WG;
+  const int rg = wid / WG, wg = wid - rg * WG;
+  if (rg >= RG) return;
   const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
   const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(n, r0 + per);
-  const int mt_total = (Mc + 7) / 8;
-  double acc[kGramTiles][NT][2];
+  double acc[TILES][NT][2];
 #pragma unroll
-  for (int t = 0; t < kGramTiles; ++t)
+  for (int t = 0; t < TILES; ++t)
 #pragma unroll
     for (int u = 0; u < NT; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
-  int acol[kGramTiles];
-  bool aon[kGramTiles];
+  int acol[TILES];
+  bool aon[TILES];
 #pragma unroll
-  for (int t = 0; t < kGramTiles; ++t) {
-    acol[t] = 8 * (wid + kGramWarps * t) + (lane >> 2);
-    aon[t] = (wid + kGramWarps * t) < mt_total && acol[t] < Mc;
+  for (int t = 0; t < TILES; ++t) {
+    acol[t] = 8 * (wg + WG * t) + (lane >> 2);
+    aon[t] = (wg + WG * t) < mt_total && acol[t] < Mc;
   }
   const int kl = lane & 3;
-  for (int64_t k0 = r0; k0 < r1; k0 += 4 * kGramUnroll) {
-    double a[kGramUnroll][kGramTiles], b[kGramUnroll][NT];
+  for (int64_t k0 = r0 + 4 * UNROLL * rg; k0 < r1; k0 += 4 * UNROLL * RG) {
+    double a[UNROLL][TILES], b[UNROLL][NT];
 #pragma unroll
-    for (int s = 0; s < kGramUnroll; ++s) {
+    for (int s = 0; s < UNROLL; ++s) {
       const int64_t i = k0 + 4 * s + kl;
       const bool rin = i < r1;
 #pragma unroll
-      for (int t = 0; t < kGramTiles; ++t)
+      for (int t = 0; t < TILES; ++t)
         a[s][t] = (rin && aon[t]) ? __ldg(A + i * lda + acol[t]) : 0.0;
 #pragma unroll
       for (int u = 0; u < NT; ++u) {
@@ -83,17 +92,17 @@ __global__ void __launch_bounds__(kGramThreads, 1) k_gram(const double* __restri
       }
     }
 #pragma unroll
-    for (int s = 0; s < kGramUnroll; ++s)
+    for (int s = 0; s < UNROLL; ++s)
 #pragma unroll
-      for (int t = 0; t < kGramTiles; ++t)
-        if ((wid + kGramWarps * t) < mt_total)
+      for (int t = 0; t < TILES; ++t)
+        if ((wg + WG * t) < mt_total)
 #pragma unroll
           for (int u = 0; u < NT; ++u) dmma(acc[t][u], a[s][t], b[s][u]);
   }
-  double* out = part + (int64_t)blockIdx.x * Mc * P;
+  double* out = part + ((int64_t)blockIdx.x * RG + rg) * Mc * P;
 #pragma unroll
-  for (int t = 0; t < kGramTiles; ++t) {
-    const int mt = wid + kGramWarps * t;
+  for (int t = 0; t < TILES; ++t) {
+    const int mt = wg + WG * t;
     if (mt >= mt_total) continue;
     const int r = 8 * mt + (lane >> 2);
     if (r >= Mc) continue;
@@ -107,14 +116,38 @@ __global__ void __launch_bounds__(kGramThreads, 1) k_gram(const double* __restri
   }
 }
 
-__global__ void k_gram_reduce(const double* __restrict__ part, int nblk, int M, int P,
-                              double alpha, double beta, double* __restrict__ C, int ldc) {
-  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < M * P; x += gridDim.x * blockDim.x) {
+// Row groups of one k_gram launch (as the kernel computes them).
+inline int gram_groups(int Mc, int tiles_per_warp) {
+  const int mt = (Mc + 7) / 8;
+  const int wg = (mt + tiles_per_warp - 1) / tiles_per_warp;
+  return 2 * wg > kGramWarps ? 1 : kGramWarps / wg;
+}
+
+// Sums the blocks' partials: a block of kRedWarps warps owns 32 consecutive entries of C; warp w
+// adds the partials of blocks w, w + kRedWarps, ... (lane = entry, so each partial row is read as
+// one 256-byte segment) and the warps' sums are combined in warp order, so the result is the same
+// on every run.
+constexpr int kRedWarps = 8;
+__global__ void __launch_bounds__(kRedWarps * 32) k_gram_reduce(const double* __restrict__ part,
+                                                                int nblk, int M, int P, double alpha,
+                                                                double beta, double* __restrict__ C,
+                                                                int ldc) {
+  __shared__ double ws[kRedWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = blockIdx.x * 32 + lane;
+  const int64_t mp = (int64_t)M * P;
+  double s = 0.0;
+  if (x < mp)
+    for (int b = w; b < nblk; b += kRedWarps) s += part[b * mp + x];
+  ws[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && x < mp) {
+    double t = ws[0][lane];
+#pragma unroll
+    for (int v = 1; v < kRedWarps; ++v) t += ws[v][lane];
     const int a = x / P, c = x - a * P;
-    double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * M * P + x];
     double* o = C + a + (int64_t)c * ldc;
-    *o = beta == 0.0 ? alpha * s : alpha * s + beta * *o;
+    *o = beta == 0.0 ? alpha * t : alpha * t + beta * *o;
   }
 }
 
@@ -332,7 +365,9 @@ void set_attributes() {
 }  // namespace
 
 int64_t proj_gram_scratch(int M, int P) {
-  return (int64_t)kBlocks * std::min(M, kGramSlab) * P;
+  // blocks x row groups x Mc <= kBlocks x kGramSlab for every slab width (groups x tiles <= 96)
+  (void)M;
+  return (int64_t)kBlocks * kGramSlab * P;
 }
 
 bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, int M, int P,
@@ -343,12 +378,22 @@ bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, in
   if (n < (int64_t)nblk * 64) nblk = (int)std::max<int64_t>(1, (n + 63) / 64);
   for (int a0 = 0; a0 < M; a0 += kGramSlab) {
     const int Mc = std::min(kGramSlab, M - a0);
+    // up to 16 tiles of C: one tile per warp and eight k-steps in flight; wider: six tiles
+    const bool narrow = Mc <= 8 * kGramWarps;
+    const int nparts = nblk * gram_groups(Mc, narrow ? 1 : kGramTiles);
     note_launch();
-    if (P <= 8) k_gram<1><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
-    else k_gram<2><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+    if (narrow) {
+      if (P <= 8) k_gram<1, 1, 8><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+      else k_gram<2, 1, 8><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+    } else {
+      if (P <= 8)
+        k_gram<1, kGramTiles, kGramUnroll><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+      else
+        k_gram<2, kGramTiles, kGramUnroll><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+    }
     note_launch();
-    k_gram_reduce<<<(Mc * P + 255) / 256, 256, 0, s>>>(part, nblk, Mc, P, alpha, beta, C + a0,
-                                                        ldc);
+    k_gram_reduce<<<(Mc * P + 31) / 32, kRedWarps * 32, 0, s>>>(part, nparts, Mc, P, alpha, beta,
+                                                                 C + a0, ldc);
   }
   return true;
 }
@@ -367,7 +412,7 @@ bool proj_rows_gram(const double* A, int lda, const double* S1, int lds, double*
   else
     k_rows_gram<2><<<nblk, kThreads, fuse_smem<2>(M), s>>>(A, lda, S1, lds, W, ldw, n, M, P, part);
   note_launch();
-  k_gram_reduce<<<(M * P + 255) / 256, 256, 0, s>>>(part, nblk, M, P, 1.0, 0.0, C, ldc);
+  k_gram_reduce<<<(M * P + 31) / 32, kRedWarps * 32, 0, s>>>(part, nblk, M, P, 1.0, 0.0, C, ldc);
   return true;
 }
 
