@@ -224,18 +224,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_rows(const double* __restrict__
 // The second and third Gram-Schmidt passes over the same rows of A, fused:
 //   W <- W - A S1            (S1: M x P column-major)
 //   part[block] = A^T W      (with the updated W; this block's rows, M x P a-major)
-// A block walks chunks of 256 rows (32 warps x one 8-row tile): each warp updates its tile of W (A
-// from global memory, S1 from shared memory) and leaves the new rows in a shared copy; then every
-// warp adds A_chunk^T W_chunk to its 8-row tiles of the partial Gram product, re-reading the
-// chunk's rows of A, which the first phase has just brought into L2.  One pass over A from HBM
-// instead of two.
-constexpr int kFuseChunk = 256;
+// A block walks chunks of 128 rows (16 8-row tiles): warps w and w + 16 each form the product of
+// tile w over one half of A's columns (A from global memory, S1 from shared memory), the second
+// hands its half to the first through shared memory, which updates the tile of W and leaves the
+// new rows in a shared copy; then every warp adds A_chunk^T W_chunk to its 8-row tiles of the
+// partial Gram product, re-reading the chunk's rows of A, which the first phase has just brought
+// into L2.  One pass over A from HBM instead of two: the chunks in flight over the whole GPU
+// (148 x 128 rows of A, 58 MB at M = 384, 97 MB at M = 640) stay within L2, which 256-row chunks
+// did not (measured: 31 % L2 hits on the re-read at M = 437 with 256-row chunks).
+constexpr int kFuseChunk = 128;
 constexpr int kFuseTiles = 3;       // Gram tiles per warp: M <= 32 x 3 x 8 = 768
 constexpr int kFuseMaxM = 32 * kFuseTiles * 8;
 
 template <int NT>
 constexpr size_t fuse_smem(int M) {
-  return (size_t)(M + kFuseChunk) * (8 * NT + 4) * sizeof(double);
+  // S1 slab, chunk of W, and the second half-products of phase 1 (16 warps x 32 lanes x NT x 2)
+  return (size_t)(M + kFuseChunk) * (8 * NT + 4) * sizeof(double) +
+         (size_t)16 * 32 * NT * 2 * sizeof(double);
 }
 
 template <int NT>
@@ -248,6 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_rows_gram(const double* __restr
   constexpr int SW = 8 * NT + 4;
   double* sS = smf;               // [M][SW]
   double* sW = smf + M * SW;      // [kFuseChunk][SW]
+  double* sH = sW + kFuseChunk * SW;  // [16][32][NT][2]: phase-1 products of the upper warps
   for (int x = threadIdx.x; x < M * 8 * NT; x += blockDim.x) {
     const int a = x / (8 * NT), c = x - a * (8 * NT);
     sS[a * SW + c] = c < P ? S1[a + (int64_t)c * lds] : 0.0;
@@ -263,39 +269,51 @@ __global__ void __launch_bounds__(kThreads, 1) k_rows_gram(const double* __restr
 #pragma unroll
     for (int u = 0; u < NT; ++u) g[t][u][0] = g[t][u][1] = 0.0;
   for (int64_t c0 = r0; c0 < r1; c0 += kFuseChunk) {
-    // phase 1: this warp's 8 rows of W - A S1
-    const int64_t i = c0 + 8 * wid + (lane >> 2);
+    // phase 1: tile wid % 16 of W - A S1; warps 0-15 take A's columns [0, kh), warps 16-31
+    // [kh, M), kh a multiple of the 4 kUnroll columns one step covers
+    const int tl = wid & 15, half = wid >> 4;
+    const int kh = ((M + 1) / 2 + 4 * kUnroll - 1) / (4 * kUnroll) * (4 * kUnroll);
+    const int kb = half ? kh : 0, ke = half ? M : min(kh, M);
+    const int64_t i = c0 + 8 * tl + (lane >> 2);
     const bool rin = i < r1;
     const double* arow = A + (rin ? i : 0) * lda;
     double acc[NT][2];
 #pragma unroll
     for (int u = 0; u < NT; ++u) acc[u][0] = acc[u][1] = 0.0;
-    for (int k0 = 0; k0 < M; k0 += 4 * kUnroll) {
+    for (int k0 = kb; k0 < ke; k0 += 4 * kUnroll) {
       double a[kUnroll];
 #pragma unroll
       for (int s = 0; s < kUnroll; ++s) {
         const int k = k0 + 4 * s + kl;
-        a[s] = (rin && k < M) ? __ldg(arow + k) : 0.0;
+        a[s] = (rin && k < ke) ? __ldg(arow + k) : 0.0;
       }
 #pragma unroll
       for (int s = 0; s < kUnroll; ++s) {
         const int k = k0 + 4 * s + kl;
-        if (k0 + 4 * s < M) {
+        if (k0 + 4 * s < ke) {
 #pragma unroll
           for (int u = 0; u < NT; ++u)
-            dmma(acc[u], a[s], k < M ? sS[k * SW + 8 * u + (lane >> 2)] : 0.0);
+            dmma(acc[u], a[s], k < ke ? sS[k * SW + 8 * u + (lane >> 2)] : 0.0);
         }
       }
     }
-    const int rl = 8 * wid + (lane >> 2);
+    if (half) {
+#pragma unroll
+      for (int u = 0; u < NT; ++u)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) sH[((tl * 32 + lane) * NT + u) * 2 + j] = acc[u][j];
+    }
+    __syncthreads();
+    const int rl = 8 * tl + (lane >> 2);
 #pragma unroll
     for (int u = 0; u < NT; ++u)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int c = 8 * u + 2 * (lane & 3) + j;
+        if (half) continue;
         double wv = 0.0;
         if (rin && c < P) {
-          wv = W[i * ldw + c] - acc[u][j];
+          wv = W[i * ldw + c] - (acc[u][j] + sH[((tl * 32 + lane) * NT + u) * 2 + j]);
           W[i * ldw + c] = wv;
         }
         sW[rl * SW + c] = wv;
