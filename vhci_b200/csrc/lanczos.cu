@@ -95,15 +95,6 @@ struct LWork {
   }
 };
 
-// VHCI_PROJ=blas runs the projections through cuBLAS instead (comparison runs only).
-bool proj_blas() {
-  static const bool b = [] {
-    const char* e = std::getenv("VHCI_PROJ");
-    return e && std::string(e) == "blas";
-  }();
-  return b;
-}
-
 // Projections over the basis rows, on the FP64 tensor pipe (k_proj.cu).
 // C (M x P, column-major) = alpha A^T B + beta C, A n x M and B n x P row-major.  On a sharded
 // context the n rows are this rank's block and the partial product is summed over the ranks
@@ -120,14 +111,9 @@ int gemm_gram(vhci_ctx* c, LWork& w, const double* A, int lda, const double* B, 
     out = w.gtmp.p;
     ldo = M;
   }
-  if (proj_blas()) {
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, M, P, (int)n, &alpha, A, lda, B, ldb, &beta,
-                    out, ldo));
-  } else {
-    VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
-    if (!proj_gram(A, lda, B, ldb, n, M, P, alpha, beta, out, ldo, w.gpart.p, c->st))
-      return fail(c, VHCI_E_INPUT, "projection with more than 16 right-hand columns");
-  }
+  VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
+  if (!proj_gram(A, lda, B, ldb, n, M, P, alpha, beta, out, ldo, w.gpart.p, c->st))
+    return fail(c, VHCI_E_INPUT, "projection with more than 16 right-hand columns");
   if (sh) {
     VTRY(comm_sum(c, out, (int64_t)M * P));
     VCK(cudaMemcpy2DAsync(C, ldc * sizeof(double), out, M * sizeof(double), M * sizeof(double), P,
@@ -140,11 +126,7 @@ int gemm_gram(vhci_ctx* c, LWork& w, const double* A, int lda, const double* B, 
 int gemm_rows(vhci_ctx* c, const double* A, int lda, const double* S, int lds, int64_t n, int M,
               int P, double alpha, double beta, double* Out, int ldo) {
   if (n <= 0 || P <= 0) return VHCI_OK;
-  if (proj_blas()) {
-    VBL(cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, P, (int)n, M, &alpha, S, lds, A, lda, &beta,
-                    Out, ldo));
-    return VHCI_OK;
-  }
+  (void)c;
   proj_rows(A, lda, S, lds, n, M, P, alpha, beta, Out, ldo, c->st);
   return VHCI_OK;
 }
@@ -153,24 +135,22 @@ int gemm_rows(vhci_ctx* c, const double* A, int lda, const double* S, int lds, i
 // fused into one pass over Q's rows when the shapes allow (k_proj.cu), else as two products.
 int gemm_rows_gram(vhci_ctx* c, LWork& w, const double* Q, int ldq, const double* S1, int lds,
                    int64_t n, int M, int P, double* W, int ldw, double* C, int ldc) {
-  if (!proj_blas()) {
-    const bool sh = is_sharded(c);
-    double* out = C;
-    int ldo = ldc;
+  const bool sh = is_sharded(c);
+  double* out = C;
+  int ldo = ldc;
+  if (sh) {
+    VCK(w.gtmp.reserve((size_t)M * P, c->st));
+    out = w.gtmp.p;
+    ldo = M;
+  }
+  VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
+  if (proj_rows_gram(Q, ldq, S1, lds, W, ldw, n, M, P, out, ldo, w.gpart.p, c->st)) {
     if (sh) {
-      VCK(w.gtmp.reserve((size_t)M * P, c->st));
-      out = w.gtmp.p;
-      ldo = M;
+      VTRY(comm_sum(c, out, (int64_t)M * P));
+      VCK(cudaMemcpy2DAsync(C, ldc * sizeof(double), out, M * sizeof(double),
+                            M * sizeof(double), P, cudaMemcpyDeviceToDevice, c->st));
     }
-    VCK(w.gpart.reserve((size_t)proj_gram_scratch(M, P), c->st));
-    if (proj_rows_gram(Q, ldq, S1, lds, W, ldw, n, M, P, out, ldo, w.gpart.p, c->st)) {
-      if (sh) {
-        VTRY(comm_sum(c, out, (int64_t)M * P));
-        VCK(cudaMemcpy2DAsync(C, ldc * sizeof(double), out, M * sizeof(double),
-                              M * sizeof(double), P, cudaMemcpyDeviceToDevice, c->st));
-      }
-      return VHCI_OK;
-    }
+    return VHCI_OK;
   }
   VTRY(gemm_rows(c, Q, ldq, S1, lds, n, M, P, -1.0, 1.0, W, ldw));
   return gemm_gram(c, w, Q, ldq, W, ldw, n, M, P, 1.0, 0.0, C, ldc);
