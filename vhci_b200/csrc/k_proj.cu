@@ -49,16 +49,16 @@ constexpr int kGramUnroll = 2;
 // rows in steps of 4 UNROLL rows, so a narrow C (few tiles) still keeps every warp streaming.
 // When a group would need more than half the warps, all 16 form one group.
 // Group r of block x writes its partial to part[x * groups + r] (Mc x P, a-major).
-template <int NT, int TILES, int UNROLL>
-__global__ void __launch_bounds__(kGramThreads, 1) k_gram(const double* __restrict__ A, int lda,
-                                                      const double* __restrict__ B, int ldb,
-                                                      int64_t n, int Mc, int P,
-                                                      double* __restrict__ part) {
+template <int NT, int TILES, int UNROLL, int NWARP>
+__global__ void __launch_bounds__(NWARP * 32, 1) k_gram(const double* __restrict__ A, int lda,
+                                                    const double* __restrict__ B, int ldb,
+                                                    int64_t n, int Mc, int P,
+                                                    double* __restrict__ part) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int mt_total = (Mc + 7) / 8;
   int WG = (mt_total + TILES - 1) / TILES;
-  if (2 * WG > kGramWarps) WG = kGramWarps;  // one group: spread the tiles over all warps
-  const int RG = kGramWarps / WG;
+  if (2 * WG > NWARP) WG = NWARP;  // one group: spread the tiles over all warps
+  const int RG = NWARP / WG;
   const int rg = wid / WG, wg = wid - rg * WG;
   if (rg >= RG) return;
   const int64_t per = ((n + gridDim.x - 1) / gridDim.x + 3) & ~int64_t(3);
@@ -117,10 +117,10 @@ __global__ void __launch_bounds__(kGramThreads, 1) k_gram(const double* __restri
 }
 
 // Row groups of one k_gram launch (as the kernel computes them).
-inline int gram_groups(int Mc, int tiles_per_warp) {
+inline int gram_groups(int Mc, int tiles_per_warp, int nwarp) {
   const int mt = (Mc + 7) / 8;
   const int wg = (mt + tiles_per_warp - 1) / tiles_per_warp;
-  return 2 * wg > kGramWarps ? 1 : kGramWarps / wg;
+  return 2 * wg > nwarp ? 1 : nwarp / wg;
 }
 
 // Sums the blocks' partials: a block of kRedWarps warps owns 32 consecutive entries of C; warp w
@@ -396,18 +396,26 @@ bool proj_gram(const double* A, int lda, const double* B, int ldb, int64_t n, in
   if (n < (int64_t)nblk * 64) nblk = (int)std::max<int64_t>(1, (n + 63) / 64);
   for (int a0 = 0; a0 < M; a0 += kGramSlab) {
     const int Mc = std::min(kGramSlab, M - a0);
-    // up to 16 tiles of C: one tile per warp and eight k-steps in flight; wider: six tiles
-    const bool narrow = Mc <= 8 * kGramWarps;
-    const int nparts = nblk * gram_groups(Mc, narrow ? 1 : kGramTiles);
+    // up to 16 tiles of C: 16 warps, one tile each, eight k-steps in flight; up to 64 tiles: 32
+    // warps, two tiles each, four k-steps; wider: 16 warps, six tiles each, two k-steps (measured
+    // on 380k rows, P = 16: 0.39 ms against 0.47 ms at M = 512 for the middle form, and 0.50
+    // against 0.55 ms at M = 672 for the wide one)
+    const int form = Mc <= 8 * kGramWarps ? 0 : (Mc <= 8 * 2 * 32 ? 1 : 2);
+    const int nparts = nblk * (form == 0   ? gram_groups(Mc, 1, kGramWarps)
+                               : form == 1 ? gram_groups(Mc, 2, 32)
+                                           : gram_groups(Mc, kGramTiles, kGramWarps));
     note_launch();
-    if (narrow) {
-      if (P <= 8) k_gram<1, 1, 8><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
-      else k_gram<2, 1, 8><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+    if (form == 0) {
+      if (P <= 8) k_gram<1, 1, 8, kGramWarps><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+      else k_gram<2, 1, 8, kGramWarps><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+    } else if (form == 1) {
+      if (P <= 8) k_gram<1, 2, 4, 32><<<nblk, 1024, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+      else k_gram<2, 2, 4, 32><<<nblk, 1024, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
     } else {
       if (P <= 8)
-        k_gram<1, kGramTiles, kGramUnroll><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+        k_gram<1, kGramTiles, kGramUnroll, kGramWarps><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
       else
-        k_gram<2, kGramTiles, kGramUnroll><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
+        k_gram<2, kGramTiles, kGramUnroll, kGramWarps><<<nblk, kGramThreads, 0, s>>>(A + a0, lda, B, ldb, n, Mc, P, part);
     }
     note_launch();
     k_gram_reduce<<<(Mc * P + 31) / 32, kRedWarps * 32, 0, s>>>(part, nparts, Mc, P, alpha, beta,

@@ -424,7 +424,7 @@ int block_lanczos(vhci_ctx* c, int k) {
   VCK(w.Yw.reserve((size_t)ld * ld, s));
   VCK(w.theta.reserve(ld, s));
   VCK(w.Xb.reserve((size_t)rb * kk, s));  // rblk rows: the block each rank gathers at the end
-  VCK(w.HXb.reserve((size_t)nl * kk, s));
+  if (mixed) VCK(w.HXb.reserve((size_t)nl * kk, s));  // the final FP64 sweep's products
   VCK(w.W.reserve((size_t)nl * b, s));
   const int nblk = residual_blocks(nl);
   VCK(w.part.reserve((size_t)nblk * kk, s));
@@ -514,12 +514,40 @@ int block_lanczos(vhci_ctx* c, int k) {
     VTRY(comm_bcast0(c, w.theta.p, m));
     const int nk = std::min(kk, m);
     VTRY(gemm_rows(c, w.Q.p, ld, w.Yw.p, ld, nl, m, nk, 1.0, 0.0, w.Xb.p, kk));
-    VTRY(gemm_rows(c, w.HQ.p, ld, w.Yw.p, ld, nl, m, nk, 1.0, 0.0, w.HXb.p, kk));
-    residual_norms(w.Xb.p, w.HXb.p, nl, kk, nk, w.theta.p, w.part.p, nblk, w.rn2.p, s);
-    VTRY(comm_sum(c, w.rn2.p, nk));
+    // Residuals from the Krylov relation H Q = Q T + W E_last^T, where W = (I - Q Q^T) H Q_last is
+    // the pending block (formed here; the restart continues from it): the residual of Ritz pair
+    // (theta_j, y_j) is W y_j[last block rows], so ||r_j||^2 = y_last^T (W^T W) y_last.  With the
+    // full (two-pass) orthogonalisation the relation holds to rounding, far below the tolerance.
+    // The whole space (m = n) or an invariant subspace (exhausted) leaves no residual.
+    const int pw = (!exhausted && m < n) ? p : 0;
+    std::fill(rn.begin(), rn.end(), 0.0);
     VCK(d2h(c, th.data(), w.theta.p, nk * sizeof(double)));
-    VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
-    VCK(cudaStreamSynchronize(s));
+    if (pw > 0) {
+      copy_cols(w.HQ.p + (m - pw), ld, w.W.p, b, nl, pw, s);
+      VCK(w.S.reserve((size_t)std::max(m, b) * pw, s));
+      VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - pw) * ld, ld, nl, m, pw, w.W.p, b,
+                          w.S.p, m));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, pw, -1.0, 1.0, w.W.p, b));
+      VCK(w.M.reserve((size_t)pw * pw, s));
+      VTRY(gemm_gram(c, w, w.W.p, b, w.W.p, b, nl, pw, pw, 1.0, 0.0, w.M.p, pw));
+      std::vector<double> G((size_t)pw * pw), Yl((size_t)pw * nk);
+      VCK(d2h(c, G.data(), w.M.p, G.size() * sizeof(double)));
+      VCK(cudaMemcpy2DAsync(Yl.data(), pw * sizeof(double), w.Yw.p + (m - pw), ld * sizeof(double),
+                            pw * sizeof(double), nk, cudaMemcpyDeviceToHost, s));
+      VCK(cudaStreamSynchronize(s));
+      for (int j = 0; j < nk; ++j) {
+        const double* y = Yl.data() + (size_t)j * pw;
+        double q = 0.0;
+        for (int a = 0; a < pw; ++a) {
+          double ga = 0.0;
+          for (int e = 0; e < pw; ++e) ga += G[(size_t)e * pw + a] * y[e];
+          q += y[a] * ga;
+        }
+        rn[j] = q;
+      }
+    } else {
+      VCK(cudaStreamSynchronize(s));
+    }
     const int keff = std::min(k, nk);
     int nconv = 0;
     double rmax = 0.0;
@@ -543,15 +571,9 @@ int block_lanczos(vhci_ctx* c, int k) {
       w.release(s);
       return VHCI_OK;
     }
-    // ---- thick restart: pending block from the last expansion, then keep the Ritz block
+    // ---- thick restart: keep the Ritz block, continue from the pending block W formed above
     t0 = now();
-    copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
-    VCK(w.S.reserve((size_t)m * p, s));
-    VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, w.W.p, b,
-                        w.S.p, m));
-    VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
     copy_cols(w.Xb.p, kk, w.Q.p, ld, nl, nk, s);
-    copy_cols(w.HXb.p, kk, w.HQ.p, ld, nl, nk, s);
     int p2 = 0;
     VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + nk, ld, &p2));
     std::vector<double> Th((size_t)ld * nk, 0.0);
