@@ -362,6 +362,114 @@ __global__ void __launch_bounds__(kThreads, 1) k_rows_gram(const double* __restr
   }
 }
 
+// SVQB factor of a small Gram matrix on the device (one warp), so that a Lanczos step needs no
+// host round trip.  S (nb x nb, column-major, nb <= 16) = W^T W.  With D = diag(S)^(-1/2) (zero for
+// a diagonal at or below 1e-28 of the largest), D S D = U L U^T by cyclic Jacobi in the parallel
+// round-robin order (nb/2 disjoint rotations per round, Golub-Van Loan's symmetric 2 x 2 Schur
+// step, at most 30 sweeps, stop when the off-diagonal square sum is below 1e-30 of the total);
+// the directions with L > 1e-12 max(L) are kept in descending order and
+// M[:, q] = D U[:, keep_q] / sqrt(L[keep_q]) (columns past the rank are zero).  W M is then
+// orthonormal.  *rank_short is set to 1 when fewer than nb directions are kept.
+__global__ void __launch_bounds__(32) k_svqb_factor(const double* __restrict__ S, int nb,
+                                                    double* __restrict__ M,
+                                                    int* __restrict__ rank_short) {
+  __shared__ double A[16][17], U[16][17], d[16], cs[8], sn[8];
+  __shared__ int pa[8], pb[8], keep[16];
+  __shared__ int stop, rr;
+  const int lane = threadIdx.x;
+  for (int x = lane; x < nb * nb; x += 32) A[x % nb][x / nb] = S[x];
+  __syncwarp();
+  if (lane == 0) {
+    double dmax = 0.0;
+    for (int i = 0; i < nb; ++i) dmax = fmax(dmax, A[i][i]);
+    for (int i = 0; i < nb; ++i) {
+      const double v = A[i][i];
+      d[i] = (v > 1e-28 * dmax && v > 1e-300) ? 1.0 / sqrt(v) : 0.0;
+    }
+  }
+  __syncwarp();
+  for (int x = lane; x < nb * nb; x += 32) {
+    const int i = x % nb, j = x / nb;
+    A[i][j] *= d[i] * d[j];
+    U[i][j] = i == j ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  const int N = (nb + 1) & ~1;  // players of the round-robin (one idle index when nb is odd)
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    if (lane == 0) {
+      double off = 0.0, tot = 0.0;
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) {
+          tot += A[i][j] * A[i][j];
+          if (i != j) off += A[i][j] * A[i][j];
+        }
+      stop = (off <= 1e-30 * tot || off == 0.0) ? 1 : 0;
+    }
+    __syncwarp();
+    if (stop) break;
+    for (int round = 0; round < N - 1; ++round) {
+      if (lane < N / 2) {
+        int a = lane == 0 ? N - 1 : (lane + round) % (N - 1);
+        int b = lane == 0 ? round % (N - 1) : (N - 1 - lane + round) % (N - 1);
+        if (a > b) { const int t = a; a = b; b = t; }
+        double c = 1.0, sgn = 0.0;
+        if (b < nb) {
+          const double apq = A[a][b];
+          if (fabs(apq) >= 1e-300) {
+            const double theta = (A[b][b] - A[a][a]) / (2.0 * apq);
+            const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            sgn = t * c;
+          }
+        }
+        pa[lane] = a; pb[lane] = b; cs[lane] = c; sn[lane] = sgn;
+      }
+      __syncwarp();
+      for (int x = lane; x < (N / 2) * nb; x += 32) {  // rows a, b
+        const int t = x / nb, k = x % nb, a = pa[t], b = pb[t];
+        if (b >= nb) continue;
+        const double ra = A[a][k], rb = A[b][k];
+        A[a][k] = cs[t] * ra - sn[t] * rb;
+        A[b][k] = sn[t] * ra + cs[t] * rb;
+      }
+      __syncwarp();
+      for (int x = lane; x < (N / 2) * nb; x += 32) {  // columns a, b of A and U
+        const int t = x / nb, k = x % nb, a = pa[t], b = pb[t];
+        if (b >= nb) continue;
+        const double ca = A[k][a], cb = A[k][b];
+        A[k][a] = cs[t] * ca - sn[t] * cb;
+        A[k][b] = sn[t] * ca + cs[t] * cb;
+        const double ua = U[k][a], ub = U[k][b];
+        U[k][a] = cs[t] * ua - sn[t] * ub;
+        U[k][b] = sn[t] * ua + cs[t] * ub;
+      }
+      __syncwarp();
+    }
+  }
+  if (lane == 0) {
+    // descending eigenvalues above 1e-12 of the largest
+    int ord[16];
+    for (int i = 0; i < nb; ++i) ord[i] = i;
+    for (int i = 1; i < nb; ++i)
+      for (int j = i; j > 0 && A[ord[j]][ord[j]] > A[ord[j - 1]][ord[j - 1]]; --j) {
+        const int t = ord[j]; ord[j] = ord[j - 1]; ord[j - 1] = t;
+      }
+    const double lmax = A[ord[0]][ord[0]];
+    int r = 0;
+    for (int i = 0; i < nb; ++i) {
+      const double l = A[ord[i]][ord[i]];
+      if (l > 1e-12 * lmax && l > 0) keep[r++] = ord[i];
+    }
+    rr = r;
+    if (r < nb) *rank_short = 1;
+  }
+  __syncwarp();
+  for (int x = lane; x < nb * nb; x += 32) {
+    const int i = x % nb, q = x / nb;
+    M[x] = q < rr ? d[i] * U[i][keep[q]] / sqrt(A[keep[q]][keep[q]]) : 0.0;
+  }
+}
+
 // The dynamic shared-memory limits are set once per process to the largest size any launch uses,
 // so concurrent contexts never race on them.
 std::once_flag g_attr_once;
@@ -381,6 +489,11 @@ void set_attributes() {
 }
 
 }  // namespace
+
+void svqb_factor(const double* S, int nb, double* M, int* rank_short, cudaStream_t s) {
+  note_launch();
+  k_svqb_factor<<<1, 32, 0, s>>>(S, nb, M, rank_short);
+}
 
 int64_t proj_gram_scratch(int M, int P) {
   // blocks x row groups x Mc <= kBlocks x kGramSlab for every slab width (groups x tiles <= 96)

@@ -86,12 +86,13 @@ void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std::vecto
 struct LWork {
   DBuf<double> Q, HQ, T, Yw, theta, Xb, HXb, W, S, M, part, rn2, Xc, gpart, Xg, gtmp;
   DBuf<float> Xf, Xgf;  // FP32 copies of the vector block (mixed precision)
+  DBuf<int> short_flag;   // set by the device SVQB when a block loses rank
   bool exact = false;   // mixed precision: products with FP64 gathers (the final sweep)
   void release(cudaStream_t s) {
     Q.release(s); HQ.release(s); T.release(s); Yw.release(s); theta.release(s); Xb.release(s);
     HXb.release(s); W.release(s); S.release(s); M.release(s); part.release(s); rn2.release(s);
     Xc.release(s); gpart.release(s); Xg.release(s); gtmp.release(s); Xf.release(s);
-    Xgf.release(s);
+    Xgf.release(s); short_flag.release(s);
   }
 };
 
@@ -209,6 +210,18 @@ int svqb_small(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb
   VTRY(gemm_rows(c, B, ld, w.M.p, nb, (int)n, nb, rr, 1.0, 0.0, out, ldo));
   *r = rr;
   return VHCI_OK;
+}
+
+// svqb_small without the host round trip: the factor is formed on the device (svqb_factor) and
+// the block is assumed to keep its full rank nb, so nothing waits for the result; a lost
+// direction sets w.short_flag, which the caller reads at its next synchronisation.
+int svqb_dev(vhci_ctx* c, LWork& w, int64_t n, const double* B, int ld, int nb, double* out,
+             int ldo) {
+  VCK(w.S.reserve((size_t)nb * nb, c->st));
+  VTRY(gemm_gram(c, w, B, ld, B, ld, (int)n, nb, nb, 1.0, 0.0, w.S.p, nb));
+  VCK(w.M.reserve((size_t)nb * nb, c->st));
+  svqb_factor(w.S.p, nb, w.M.p, w.short_flag.p, c->st);
+  return gemm_rows(c, B, ld, w.M.p, nb, (int)n, nb, nb, 1.0, 0.0, out, ldo);
 }
 
 // Y = H X for a block of the held rows: X is first copied to a compact rows x b buffer so the SpMM
@@ -391,7 +404,15 @@ int block_lanczos_lean(vhci_ctx* c, int k);
 // Relative residual tolerance of the FP32-gather eigensolve in mixed precision.
 constexpr double kMixedTol = 1e-7;
 
-int block_lanczos(vhci_ctx* c, int k) {
+int block_lanczos_impl(vhci_ctx* c, int k, bool dev_svqb);
+
+// The block orthonormalisation of each step runs on the device (no host round trip per step) when
+// the basis is much larger than the subspace, where a block losing rank does not happen in
+// practice; if one does, the eigensolve is redone with the host factorisation, which drops the
+// lost directions.
+int block_lanczos(vhci_ctx* c, int k) { return block_lanczos_impl(c, k, true); }
+
+int block_lanczos_impl(vhci_ctx* c, int k, bool dev_svqb) {
   const int64_t n = c->n;
   // rows held by this rank (all n unless sharded)
   const int64_t nl = c->nrow, r0 = c->row0, rb = std::max(c->rblk, nl);
@@ -408,6 +429,7 @@ int block_lanczos(vhci_ctx* c, int k) {
   if (const char* e = std::getenv("VHCI_LANCZOS_SPAN")) span = std::max(2, std::min(8, std::atoi(e)));
   if (lanczos_bytes(n, nl, k, span, b) + 1e9 > avail) return block_lanczos_lean(c, k);
   const int mmax = (int)std::min<int64_t>(n, (int64_t)span * kk + 2 * b);
+  const bool dev = dev_svqb && n >= 8 * (int64_t)mmax;
   // row stride padded to whole 128-byte lines so every b-column gather touches whole L2 lines
   const int ld = (mmax + b + 15) / 16 * 16;
   // mixed precision: the FP32-gather products carry rounding noise of about 1e-8 of |theta|, so
@@ -429,6 +451,8 @@ int block_lanczos(vhci_ctx* c, int k) {
   const int nblk = residual_blocks(nl);
   VCK(w.part.reserve((size_t)nblk * kk, s));
   VCK(w.rn2.reserve(kk, s));
+  VCK(w.short_flag.reserve(1, s));
+  VCK(cudaMemsetAsync(w.short_flag.p, 0, sizeof(int), s));
   fill_zero(w.Q.p, nl * (int64_t)ld, s);
   VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));
 
@@ -497,8 +521,9 @@ int block_lanczos(vhci_ctx* c, int k) {
       VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, w.W.p, b,
                           w.S.p, m));
       VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
-      int p2 = 0;
-      VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + m, ld, &p2));
+      int p2 = p;
+      if (dev) VTRY(svqb_dev(c, w, nl, w.W.p, b, p, w.Q.p + m, ld));
+      else VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + m, ld, &p2));
       t_orth += msince(t0);
       p = p2;
       if (p == 0) { exhausted = true; break; }
@@ -509,6 +534,15 @@ int block_lanczos(vhci_ctx* c, int k) {
     VCK(cudaMemcpy2DAsync(w.Yw.p, ld * sizeof(double), w.T.p, ld * sizeof(double),
                           m * sizeof(double), m, cudaMemcpyDeviceToDevice, s));
     VTRY(syevd_l(c, w.Yw.p, m, ld, w.theta.p));
+    if (dev) {  // a block that lost rank on the device: redo with the host factorisation
+      int short_rank = 0;
+      VCK(d2h(c, &short_rank, w.short_flag.p, sizeof(int)));
+      VCK(cudaStreamSynchronize(s));
+      if (short_rank) {
+        w.release(s);
+        return block_lanczos_impl(c, k, false);
+      }
+    }
     // one projected solution for every rank: rank 0's
     VTRY(comm_bcast0(c, w.Yw.p, (int64_t)ld * m));
     VTRY(comm_bcast0(c, w.theta.p, m));
@@ -574,8 +608,9 @@ int block_lanczos(vhci_ctx* c, int k) {
     // ---- thick restart: keep the Ritz block, continue from the pending block W formed above
     t0 = now();
     copy_cols(w.Xb.p, kk, w.Q.p, ld, nl, nk, s);
-    int p2 = 0;
-    VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + nk, ld, &p2));
+    int p2 = p;
+    if (dev) VTRY(svqb_dev(c, w, nl, w.W.p, b, p, w.Q.p + nk, ld));
+    else VTRY(svqb_small(c, w, nl, w.W.p, b, p, w.Q.p + nk, ld, &p2));
     std::vector<double> Th((size_t)ld * nk, 0.0);
     for (int j = 0; j < nk; ++j) Th[(size_t)j * ld + j] = th[j];
     VCK(cudaMemsetAsync(w.T.p, 0, (size_t)ld * ld * sizeof(double), s));

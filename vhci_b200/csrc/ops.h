@@ -164,6 +164,10 @@ void proj_rows(const double* A, int lda, const double* S, int lds, int64_t n, in
 // (false, nothing launched, otherwise); part holds proj_gram_scratch(M, P) doubles.
 bool proj_rows_gram(const double* A, int lda, const double* S1, int lds, double* W, int ldw,
                     int64_t n, int M, int P, double* C, int ldc, double* part, cudaStream_t s);
+// SVQB factor M (nb x nb, column-major) of the Gram matrix S = W^T W (nb <= 16) on the device:
+// W M is orthonormal over the directions above 1e-12 of the largest, further columns of M are
+// zero and *rank_short is set to 1 when there are any.
+void svqb_factor(const double* S, int nb, double* M, int* rank_short, cudaStream_t s);
 
 // ---- PT2 (k_pt2.cu) ----
 void pt2_count(const uint64_t* keys, int64_t n, KeyLayout L, HashView pert, ConnDev cd,
