@@ -63,10 +63,9 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     VCK(cudaMemsetAsync(acount.p, 0, std::max<int64_t>(NA, 1) * sizeof(int32_t), s));
     pt2_count(c->keys.p, n, L, pv, conn_view(c), A0, A1, acount.p, s);
     exclusive_scan_i32(acount.p, arow.p, NA, tmp.p, s);
-    std::vector<int64_t> arow_h(NA + 1);
-    VCK(d2h(c, arow_h.data(), arow.p, (NA + 1) * sizeof(int64_t)));
+    int64_t total = 0;
+    VCK(d2h(c, &total, arow.p + NA, sizeof(int64_t)));
     VCK(cudaStreamSynchronize(s));
-    const int64_t total = arow_h[NA];
     c->stats.pt2_entries += total;
     // chunk the perturber range so one chunk's entries fit the budget
     size_t freeb = 0, totb = 0;
@@ -74,8 +73,20 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     // entries (12 bytes) plus, in the worst case, the same again as scratch for long-row ordering
     int64_t budget = c->o.pt2_chunk > 0 ? c->o.pt2_chunk : (int64_t)(freeb * 0.4 / 12.0);
     budget = std::max<int64_t>(budget, 1 << 20);
-    // chunk bounds in perturber indices; arow_h is indexed from A0
+    // chunk bounds in perturber indices (arow_h is indexed from A0); one chunk needs only the total,
+    // several the host copy of the row offsets
     std::vector<int64_t> bounds{A0};
+    std::vector<int64_t> arow_h;
+    if (total <= budget) {
+      bounds.push_back(A1);
+    } else {
+      arow_h.resize(NA + 1);
+      VCK(d2h(c, arow_h.data(), arow.p, (NA + 1) * sizeof(int64_t)));
+      VCK(cudaStreamSynchronize(s));
+    }
+    auto chunk_entries = [&](int64_t a0, int64_t a1) {
+      return arow_h.empty() ? total : arow_h[a1 - A0] - arow_h[a0 - A0];
+    };
     while (bounds.back() < A1) {
       const int64_t a0 = bounds.back();
       const int64_t lim = arow_h[a0 - A0] + budget;
@@ -89,7 +100,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     const int64_t maxchunk = [&] {
       int64_t mx = 0;
       for (size_t q = 1; q < bounds.size(); ++q)
-        mx = std::max(mx, arow_h[bounds[q] - A0] - arow_h[bounds[q - 1] - A0]);
+        mx = std::max(mx, chunk_entries(bounds[q - 1], bounds[q]));
       return mx;
     }();
     VCK(ecol.reserve(std::max<int64_t>(maxchunk, 1), s));
@@ -104,33 +115,34 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     DBuf<int64_t> crow, lrow_d, loff_d;
     DBuf<int32_t> lcol;
     DBuf<double> lval;
+    DBuf<unsigned long long> lcnt;
+    VCK(lcnt.reserve(2, s));
     for (size_t q = 1; q < bounds.size(); ++q) {
-      const int64_t a0 = bounds[q - 1], a1 = bounds[q];
-      VCK(crow.reserve(a1 - a0 + 1, s));
-      std::vector<int64_t> cr(a1 - a0 + 1);
-      for (int64_t a = a0; a <= a1; ++a) cr[a - a0] = arow_h[a - A0] - arow_h[a0 - A0];
-      VCK(h2d(c, crow.p, cr.data(), cr.size() * sizeof(int64_t)));
-      VCK(cudaMemsetAsync(acount.p, 0, (a1 - a0) * sizeof(int32_t), s));
+      const int64_t a0 = bounds[q - 1], a1 = bounds[q], na = a1 - a0;
+      // this chunk's row offsets, rebased on the device
+      VCK(crow.reserve(na + 1, s));
+      pt2_rebase_rows(arow.p + (a0 - A0), na, crow.p, s);
+      // rows too long for one warp's ordering, listed on the device; only their count and
+      // entries come back, to size the scratch and the launch
+      const int64_t maxlong = std::min<int64_t>(na, chunk_entries(a0, a1) / pt2_sort_long_min() + 1);
+      VCK(lrow_d.reserve(std::max<int64_t>(maxlong, 1), s));
+      VCK(loff_d.reserve(std::max<int64_t>(maxlong, 1), s));
+      VCK(cudaMemsetAsync(lcnt.p, 0, 2 * sizeof(unsigned long long), s));
+      pt2_list_long(crow.p, na, lrow_d.p, loff_d.p, lcnt.p, s);
+      unsigned long long lc[2] = {0, 0};
+      VCK(d2h(c, lc, lcnt.p, sizeof(lc)));
+      VCK(cudaStreamSynchronize(s));
+      VCK(cudaMemsetAsync(acount.p, 0, na * sizeof(int32_t), s));
       pt2_fill(c->keys.p, n, L, pv, conn_view(c), a0, a1, crow.p, acount.p, ecol.p, eval.p, s);
       // fixed entry order per row (the fill's atomics leave it arbitrary): short rows by one warp
-      // each, long rows (listed here from the host copy of the row offsets) by one block each
-      pt2_sort_rows(crow.p, a1 - a0, ecol.p, eval.p, s);
-      std::vector<int64_t> lrows, loff;
-      int64_t ltot = 0;
-      for (int64_t a = a0; a < a1; ++a) {
-        const int64_t len = cr[a - a0 + 1] - cr[a - a0];
-        if (len >= pt2_sort_long_min()) { lrows.push_back(a - a0); loff.push_back(ltot); ltot += len; }
-      }
-      if (!lrows.empty()) {
-        VCK(lrow_d.reserve(lrows.size(), s));
-        VCK(loff_d.reserve(loff.size(), s));
-        VCK(lcol.reserve(ltot, s));
-        VCK(lval.reserve(ltot, s));
-        VCK(h2d(c, lrow_d.p, lrows.data(), lrows.size() * sizeof(int64_t)));
-        VCK(h2d(c, loff_d.p, loff.data(), loff.size() * sizeof(int64_t)));
-        for (size_t q0 = 0; q0 < lrows.size(); q0 += 65535)
+      // each, long rows by one block each
+      pt2_sort_rows(crow.p, na, ecol.p, eval.p, s);
+      if (lc[0] > 0) {
+        VCK(lcol.reserve((int64_t)lc[1], s));
+        VCK(lval.reserve((int64_t)lc[1], s));
+        for (int64_t q0 = 0; q0 < (int64_t)lc[0]; q0 += 65535)
           pt2_sort_long(crow.p, lrow_d.p + q0, loff_d.p + q0,
-                        (int)std::min<size_t>(65535, lrows.size() - q0), ecol.p, eval.p, lcol.p,
+                        (int)std::min<int64_t>(65535, (int64_t)lc[0] - q0), ecol.p, eval.p, lcol.p,
                         lval.p, s);
       }
       EventPair ev_r0r1;
@@ -146,7 +158,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, r0, r1);
       c->stats.ms_pt2_reduce += ms;
-      const int64_t ent = cr.back();
+      const int64_t ent = chunk_entries(a0, a1);
       c->stats.pt2_reduce_bytes += ent * (4 + 8) + ent * (int64_t)nopt * 8 + (a1 - a0) * (8 + 8 * L.W);
     }
     VTRY(comm_sum(c, dEd.p, nopt));  // the ranks' shares of the perturber sum
@@ -158,7 +170,7 @@ int pt2(vhci_ctx* c, double eps2, double* dE_out, int64_t* n_pert) {
     if (fl & kFlagTableFull) return fail(c, VHCI_E_TABLE_FULL, "perturber hash full");
     pkeys.release(s); pslots.release(s); acount.release(s); arow.release(s); tmp.release(s);
     ecol.release(s); eval.release(s); part.release(s); dEd.release(s); Ed.release(s); crow.release(s);
-    lrow_d.release(s); loff_d.release(s); lcol.release(s); lval.release(s);
+    lrow_d.release(s); loff_d.release(s); lcol.release(s); lval.release(s); lcnt.release(s);
   }
   for (int j = 0; j < nopt; ++j) {
     c->E[j] += dE[j];

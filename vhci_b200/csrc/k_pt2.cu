@@ -269,7 +269,46 @@ __global__ void __launch_bounds__(256) k_pt2_sort_long(const int64_t* __restrict
   }
 }
 
+// crow[i] = arow[i] - arow[0], i in [0, nrows]: a chunk's row offsets from the whole range's.
+__global__ void k_pt2_rebase(const int64_t* __restrict__ arow, int64_t nrows,
+                             int64_t* __restrict__ crow) {
+  const int64_t base = arow[0];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= nrows;
+       i += (int64_t)gridDim.x * blockDim.x)
+    crow[i] = arow[i] - base;
+}
+
+// Lists the rows of at least minlen entries: rows[q] and a disjoint scratch offset soff[q] of
+// the row's length, q from an atomic counter (cnt[0] rows, cnt[1] entries).  The order of the
+// list does not matter: each listed row is ordered by its own block.
+__global__ void k_pt2_list_long(const int64_t* __restrict__ arowptr, int64_t nrows, int minlen,
+                                int64_t* __restrict__ rows, int64_t* __restrict__ soff,
+                                unsigned long long* __restrict__ cnt) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t len = arowptr[r + 1] - arowptr[r];
+    if (len >= minlen) {
+      const unsigned long long q = atomicAdd(cnt, 1ull);
+      rows[q] = r;
+      soff[q] = (int64_t)atomicAdd(cnt + 1, (unsigned long long)len);
+    }
+  }
+}
+
 }  // namespace
+
+void pt2_rebase_rows(const int64_t* arow, int64_t nrows, int64_t* crow, cudaStream_t s) {
+  note_launch();
+  k_pt2_rebase<<<grid_for(nrows + 1, 256, 148 * 8), 256, 0, s>>>(arow, nrows, crow);
+}
+
+void pt2_list_long(const int64_t* arowptr, int64_t nrows, int64_t* rows, int64_t* soff,
+                   unsigned long long* cnt, cudaStream_t s) {
+  if (nrows <= 0) return;
+  note_launch();
+  k_pt2_list_long<<<grid_for(nrows, 256, 148 * 8), 256, 0, s>>>(arowptr, nrows, kSortWarpCap + 1,
+                                                                 rows, soff, cnt);
+}
 
 void pt2_sort_rows(const int64_t* arowptr, int64_t nrows, int32_t* ecol, double* eval,
                    cudaStream_t s) {

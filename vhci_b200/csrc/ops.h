@@ -190,6 +190,12 @@ bool pt2_en(const uint64_t* pkeys, int64_t a_lo, int64_t a_hi, KeyLayout L, Conn
 void pt2_sort_rows(const int64_t* arowptr, int64_t nrows, int32_t* ecol, double* eval,
                    cudaStream_t s);
 int pt2_sort_long_min();
+// crow[i] = arow[i] - arow[0] for i in [0, nrows]
+void pt2_rebase_rows(const int64_t* arow, int64_t nrows, int64_t* crow, cudaStream_t s);
+// rows of at least pt2_sort_long_min() entries into rows[] with disjoint scratch offsets soff[]
+// (cnt[0] += rows listed, cnt[1] += their entries; both zeroed by the caller)
+void pt2_list_long(const int64_t* arowptr, int64_t nrows, int64_t* rows, int64_t* soff,
+                   unsigned long long* cnt, cudaStream_t s);
 void pt2_sort_long(const int64_t* arowptr, const int64_t* rows, const int64_t* soff, int nlong,
                    int32_t* ecol, double* eval, int32_t* tcol, double* tval, cudaStream_t s);
 void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cudaStream_t s);
