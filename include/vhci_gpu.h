@@ -111,6 +111,9 @@ typedef struct {
                                      them, mostly from L2                                       */
   double mixed_max_residual;      /* mixed precision: largest ||H x - theta x|| / max(1, |theta|)
                                      of the Ritz pairs after the FP64 sweeps                     */
+  int64_t hbuild_incremental;     /* Hamiltonian builds that extended the stored matrix by the
+                                     rows of the newly added states (no counterpart in the
+                                     reference, which rebuilds H every heat-bath iteration)      */
 } vhci_stats;
 
 typedef void (*vhci_iter_cb)(void* user, int iteration, int64_t n_basis, double zpe);

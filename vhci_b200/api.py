@@ -117,7 +117,8 @@ class Stats(ctypes.Structure):
                 ("pt2_reduce_bytes", ctypes.c_int64), ("eig_iterations", ctypes.c_int),
                 ("hci_iterations", ctypes.c_int), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
-                ("spmm_gather_bytes", ctypes.c_int64), ("mixed_max_residual", ctypes.c_double)]
+                ("spmm_gather_bytes", ctypes.c_int64), ("mixed_max_residual", ctypes.c_double),
+                ("hbuild_incremental", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

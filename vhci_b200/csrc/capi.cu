@@ -552,6 +552,122 @@ bool dense_path(int64_t n, int k) {
   return n <= 2000 || n <= 3 * kk + 64;
 }
 
+// Incremental build: rows of the states appended since the stored matrix was built (states
+// h_prefix .. n - 1), their entries in old columns transposed into the tails of the old rows
+// (H is symmetric to the bit: each element's ladder factors come from the lower state), merged
+// into a new CSR.  The transposed entries are radix-sorted by (column, entry), so each old row's
+// tail lists its new columns in ascending order and the layout is the same on every run.
+// Returns VHCI_OK, 1 when it declines (too many entries for the 32-bit entry keys, or not enough
+// device memory to hold the old and the new matrix at once: the caller builds from scratch),
+// or an error.
+static int build_h_incremental(vhci_ctx* c) {
+  const int64_t n = c->n, n_old = c->h_prefix, nn = n - n_old;
+  cudaStream_t s = c->st;
+  const bool f = c->o.precision == 1;
+  const double vb = f ? 4.0 : 8.0;
+  VCK(cudaEventRecord(c->ev_a, s));
+  DBuf<int32_t> cnt_new, tcol, add, erow, len, col_all;
+  DBuf<int64_t> rp_new, xoff, rp_all, hist;
+  DBuf<double> tval, tdiag, val_all, diag_all;
+  DBuf<float> tvalf, valf_all;
+  DBuf<uint64_t> keys, alt;
+  DBuf<unsigned long long> kc;
+  auto release_all = [&] {
+    cnt_new.release(s); tcol.release(s); add.release(s); erow.release(s); len.release(s);
+    col_all.release(s); rp_new.release(s); xoff.release(s); rp_all.release(s); hist.release(s);
+    tval.release(s); tdiag.release(s); val_all.release(s); diag_all.release(s); tvalf.release(s);
+    valf_all.release(s); keys.release(s); alt.release(s); kc.release(s);
+  };
+  VCK(cnt_new.reserve(nn, s));
+  VCK(rp_new.reserve(nn + 1, s));
+  VCK(c->scan_tmp.reserve(std::max<int64_t>(scan_tmp_elems(n), 1), s));
+  hbuild_count(c->keys.p, n_old, nn, c->L, basis_view(c), conn_view(c), cnt_new.p, s);
+  exclusive_scan_i32(cnt_new.p, rp_new.p, nn, c->scan_tmp.p, s);
+  int64_t nnz_new = 0;
+  VCK(d2h(c, &nnz_new, rp_new.p + nn, sizeof(int64_t)));
+  VCK(cudaStreamSynchronize(s));
+  // working set: the new rows, their transposed keys (sorted through a second buffer), the entry
+  // rows, and the merged matrix (at most nnz_old + 2 nnz_new entries) beside the stored one
+  const double nnz_all_max = (double)c->nnz + 2.0 * (double)nnz_new;
+  const double need = (double)nnz_new * (4.0 + vb + 16.0 + 4.0) + nnz_all_max * (4.0 + vb) +
+                      (double)n * 40.0 + 8.0 * radix_hist_elems(nnz_new);
+  const double eig = lanczos_min_bytes(c, c->M.nstate);
+  const double old_bytes = (double)c->nnz * (4.0 + vb) + 16.0 * (double)n_old;
+  const double avail = device_available(c);
+  if (nnz_new >= 0xFFFFFFFFll || need > 0.9 * avail || nnz_all_max * (4.0 + vb) + eig > avail + old_bytes) {
+    release_all();
+    return 1;
+  }
+  VCK(tcol.reserve(std::max<int64_t>(nnz_new, 1), s));
+  if (f) VCK(tvalf.reserve(std::max<int64_t>(nnz_new, 1), s));
+  else VCK(tval.reserve(std::max<int64_t>(nnz_new, 1), s));
+  VCK(tdiag.reserve(nn, s));
+  hbuild_fill(c->keys.p, n_old, nn, c->L, basis_view(c), conn_view(c), rp_new.p, tcol.p,
+              f ? nullptr : tval.p, f ? tvalf.p : nullptr, tdiag.p, s);
+  // transposed entries: per old column counts and (column, entry) keys, sorted
+  VCK(add.reserve(n_old, s));
+  VCK(cudaMemsetAsync(add.p, 0, n_old * sizeof(int32_t), s));
+  VCK(keys.reserve(std::max<int64_t>(nnz_new, 1), s));
+  VCK(kc.reserve(1, s));
+  VCK(cudaMemsetAsync(kc.p, 0, sizeof(unsigned long long), s));
+  hmerge_cross_keys(tcol.p, nnz_new, n_old, add.p, keys.p, kc.p, s);
+  unsigned long long ncross_u = 0;
+  VCK(d2h(c, &ncross_u, kc.p, sizeof(ncross_u)));
+  VCK(cudaStreamSynchronize(s));
+  const int64_t ncross = (int64_t)ncross_u;
+  if (ncross > 0) {
+    int cbits = 1;
+    while (cbits < 32 && ((int64_t)1 << cbits) < n_old) ++cbits;
+    VCK(alt.reserve(ncross, s));
+    VCK(hist.reserve(std::max<int64_t>(radix_hist_elems(ncross), 1), s));
+    radix_sort_keys(keys.p, alt.p, ncross, 1, 32 + cbits, hist.p, s);
+  }
+  VCK(xoff.reserve(n_old + 1, s));
+  exclusive_scan_i32(add.p, xoff.p, n_old, c->scan_tmp.p, s);
+  VCK(erow.reserve(std::max<int64_t>(nnz_new, 1), s));
+  hmerge_entry_rows(rp_new.p, nn, erow.p, s);
+  // merged row pointers and arrays
+  VCK(len.reserve(n, s));
+  hmerge_lengths(c->rowptr.p, add.p, rp_new.p, n_old, nn, len.p, s);
+  VCK(rp_all.reserve(n + 1, s));
+  exclusive_scan_i32(len.p, rp_all.p, n, c->scan_tmp.p, s);
+  const int64_t nnz_all = c->nnz + nnz_new + ncross;
+  VCK(col_all.reserve(std::max<int64_t>(nnz_all, 1), s));
+  if (f) VCK(valf_all.reserve(std::max<int64_t>(nnz_all, 1), s));
+  else VCK(val_all.reserve(std::max<int64_t>(nnz_all, 1), s));
+  VCK(diag_all.reserve(n, s));
+  hmerge_copy_rows(c->rowptr.p, c->col.p, f ? nullptr : c->val.p, f ? c->valf.p : nullptr, n_old,
+                   rp_all.p, col_all.p, val_all.p, valf_all.p, s);
+  hmerge_copy_rows(rp_new.p, tcol.p, f ? nullptr : tval.p, f ? tvalf.p : nullptr, nn,
+                   rp_all.p + n_old, col_all.p, val_all.p, valf_all.p, s);
+  hmerge_cross_scatter(keys.p, ncross, xoff.p, c->rowptr.p, rp_all.p, erow.p,
+                       f ? nullptr : tval.p, f ? tvalf.p : nullptr, n_old, col_all.p, val_all.p,
+                       valf_all.p, s);
+  VCK(cudaMemcpyAsync(diag_all.p, c->diag.p, n_old * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  VCK(cudaMemcpyAsync(diag_all.p + n_old, tdiag.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  // the merged matrix replaces the stored one (the old arrays leave with the temporaries)
+  std::swap(c->rowptr.p, rp_all.p); std::swap(c->rowptr.cap, rp_all.cap);
+  std::swap(c->col.p, col_all.p); std::swap(c->col.cap, col_all.cap);
+  if (f) { std::swap(c->valf.p, valf_all.p); std::swap(c->valf.cap, valf_all.cap); }
+  else { std::swap(c->val.p, val_all.p); std::swap(c->val.cap, val_all.cap); }
+  std::swap(c->diag.p, diag_all.p); std::swap(c->diag.cap, diag_all.cap);
+  release_all();
+  c->nnz = nnz_all;
+  c->row0 = 0;
+  c->nrow = n;
+  c->rblk = n;
+  VTRY(build_panels(c));
+  VCK(cudaEventRecord(c->ev_b, s));
+  VCK(cudaEventSynchronize(c->ev_b));
+  VCK(cudaGetLastError());
+  c->stats.ms_hbuild += event_ms(c);
+  c->stats.hbuild_probes += 2 * nn * (int64_t)c->conn.groups.size();
+  c->stats.hbuild_incremental += 1;
+  c->h_prefix = n;
+  c->h_valid = true;
+  return VHCI_OK;
+}
+
 int build_h(vhci_ctx* c, bool all_rows) {
   const int64_t n = c->n;
   c->npanel = 0;
@@ -571,6 +687,11 @@ int build_h(vhci_ctx* c, bool all_rows) {
     c->rblk = n;
   }
   const int64_t r0 = c->row0, nr = c->nrow;
+  if (!c->h_rows && c->h_prefix > 0 && c->h_prefix < n) {
+    const int r = build_h_incremental(c);
+    if (r != 1) return r;
+  }
+  c->h_prefix = 0;
   VCK(cudaEventRecord(c->ev_a, c->st));
   VCK(c->rowcnt.reserve(std::max<int64_t>(nr, 1), c->st));
   VCK(c->rowptr.reserve(nr + 1, c->st));
@@ -617,6 +738,7 @@ int build_h(vhci_ctx* c, bool all_rows) {
   c->stats.hbuild_probes += 2 * nr * (int64_t)c->conn.groups.size();
   c->nnz = nnz;
   c->h_valid = true;
+  c->h_prefix = c->h_rows ? 0 : n;
   return VHCI_OK;
 }
 
@@ -824,6 +946,7 @@ vhci_status vhci_set_basis(vhci_ctx* c, const uint8_t* quanta, int64_t n) {
   int fl = 0;
   VTRY(read_flags(c, &fl));
   c->h_valid = false;
+  c->h_prefix = 0;
   c->npanel = 0;
   c->nvec = 0;
   c->x_rows = 0;
@@ -939,6 +1062,7 @@ vhci_status vhci_set_comm(vhci_ctx* c, const vhci_comm* comm) {
     c->comm = *comm;
   }
   c->h_valid = false;  // the held matrix's rows follow the sharding
+  c->h_prefix = 0;
   return VHCI_OK;
 }
 

@@ -112,6 +112,9 @@ struct vhci_ctx {
   // Hamiltonian (off-diagonal CSR + FP64 diagonal)
   bool h_valid = false;
   int64_t nnz = 0;
+  // the stored (whole, unsharded) matrix covers the first h_prefix states of the basis; states
+  // appended since need only their own rows (incremental build)
+  int64_t h_prefix = 0;
   vhci::DBuf<int32_t> rowcnt;
   vhci::DBuf<int64_t> rowptr;
   vhci::DBuf<int32_t> col;

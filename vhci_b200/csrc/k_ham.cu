@@ -565,4 +565,120 @@ void reduce_parts(const double* part, int nblk, int nopt, double* out_accum, cud
   note_launch(); k_sum_parts<<<(nopt + 255) / 256, 256, 0, s>>>(part, nblk, nopt, out_accum, 1);
 }
 
+// ---- incremental build: the stored matrix of the first n_old states, extended by the rows of
+// the states appended since (H is symmetric to the bit, so the new columns of the old rows are
+// the new rows' entries transposed) ----
+namespace {
+
+// add[c] += 1 for every new-row entry in an old column c, and the transposed entries' keys
+// (c << 32 | entry index) compacted through cnt (their order is fixed by the sort that follows)
+__global__ void k_cross_keys(const int32_t* __restrict__ col, int64_t nnz, int64_t n_old,
+                             int32_t* __restrict__ add, uint64_t* __restrict__ keys,
+                             unsigned long long* __restrict__ cnt) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = col[e];
+    if (c < n_old) {
+      atomicAdd(add + c, 1);
+      keys[atomicAdd(cnt, 1ull)] = ((uint64_t)(uint32_t)c << 32) | (uint64_t)e;
+    }
+  }
+}
+
+// entry -> row of the new rows' CSR (one warp per row)
+__global__ void k_entry_rows(const int64_t* __restrict__ rp, int64_t nrows, int32_t* __restrict__ erow) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows;
+       r += ((int64_t)gridDim.x * blockDim.x) >> 5)
+    for (int64_t e = rp[r] + lane; e < rp[r + 1]; e += 32) erow[e] = (int32_t)r;
+}
+
+// merged row lengths: old rows keep their entries and gain add[i]; new rows as built
+__global__ void k_merge_len(const int64_t* __restrict__ rp_old, const int32_t* __restrict__ add,
+                            const int64_t* __restrict__ rp_new, int64_t n_old, int64_t nn,
+                            int32_t* __restrict__ len) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_old + nn;
+       i += (int64_t)gridDim.x * blockDim.x)
+    len[i] = i < n_old ? (int32_t)(rp_old[i + 1] - rp_old[i]) + add[i]
+                       : (int32_t)(rp_new[i - n_old + 1] - rp_new[i - n_old]);
+}
+
+// rows [rs[i], rs[i+1]) copied to rd[i].. (one warp per row)
+template <typename VT>
+__global__ void k_copy_rows(const int64_t* __restrict__ rs, const int32_t* __restrict__ cs,
+                            const VT* __restrict__ vs, int64_t nrows, const int64_t* __restrict__ rd,
+                            int32_t* __restrict__ cd, VT* __restrict__ vd) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows;
+       r += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t b = rs[r], m = rs[r + 1] - b, d = rd[r];
+    for (int64_t t = lane; t < m; t += 32) {
+      cd[d + t] = cs[b + t];
+      vd[d + t] = vs[b + t];
+    }
+  }
+}
+
+// the sorted transposed entries to the tails of the old rows: key t of column c goes to position
+// rp_all[c] + (old length of c) + (t - first key of c), as column n_old + (its new row)
+template <typename VT>
+__global__ void k_cross_scatter(const uint64_t* __restrict__ keys, int64_t ncross,
+                                const int64_t* __restrict__ xoff, const int64_t* __restrict__ rp_old,
+                                const int64_t* __restrict__ rp_all, const int32_t* __restrict__ erow,
+                                const VT* __restrict__ vnew, int64_t n_old, int32_t* __restrict__ cd,
+                                VT* __restrict__ vd) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ncross;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[t];
+    const int64_t c = (int64_t)(k >> 32), e = (int64_t)(k & 0xffffffffull);
+    const int64_t pos = rp_all[c] + (rp_old[c + 1] - rp_old[c]) + (t - xoff[c]);
+    cd[pos] = (int32_t)(n_old + erow[e]);
+    vd[pos] = vnew[e];
+  }
+}
+
+}  // namespace
+
+void hmerge_cross_keys(const int32_t* col_new, int64_t nnz_new, int64_t n_old, int32_t* add,
+                       uint64_t* keys, unsigned long long* cnt, cudaStream_t s) {
+  if (nnz_new <= 0) return;
+  note_launch();
+  k_cross_keys<<<grid_for(nnz_new, 256, 148 * 8), 256, 0, s>>>(col_new, nnz_new, n_old, add, keys, cnt);
+}
+
+void hmerge_entry_rows(const int64_t* rp_new, int64_t nn, int32_t* erow, cudaStream_t s) {
+  if (nn <= 0) return;
+  note_launch();
+  k_entry_rows<<<grid_for(nn * 32, 256, 148 * 8), 256, 0, s>>>(rp_new, nn, erow);
+}
+
+void hmerge_lengths(const int64_t* rp_old, const int32_t* add, const int64_t* rp_new, int64_t n_old,
+                    int64_t nn, int32_t* len, cudaStream_t s) {
+  note_launch();
+  k_merge_len<<<grid_for(n_old + nn, 256, 148 * 8), 256, 0, s>>>(rp_old, add, rp_new, n_old, nn, len);
+}
+
+void hmerge_copy_rows(const int64_t* rs, const int32_t* cs, const double* vs, const float* vsf,
+                      int64_t nrows, const int64_t* rd, int32_t* cd, double* vd, float* vdf,
+                      cudaStream_t s) {
+  if (nrows <= 0) return;
+  note_launch();
+  const int g = grid_for(nrows * 32, 256, 148 * 8);
+  if (vsf) k_copy_rows<float><<<g, 256, 0, s>>>(rs, cs, vsf, nrows, rd, cd, vdf);
+  else k_copy_rows<double><<<g, 256, 0, s>>>(rs, cs, vs, nrows, rd, cd, vd);
+}
+
+void hmerge_cross_scatter(const uint64_t* keys, int64_t ncross, const int64_t* xoff,
+                          const int64_t* rp_old, const int64_t* rp_all, const int32_t* erow,
+                          const double* vnew, const float* vnewf, int64_t n_old, int32_t* cd,
+                          double* vd, float* vdf, cudaStream_t s) {
+  if (ncross <= 0) return;
+  note_launch();
+  const int g = grid_for(ncross, 256, 148 * 8);
+  if (vnewf)
+    k_cross_scatter<float><<<g, 256, 0, s>>>(keys, ncross, xoff, rp_old, rp_all, erow, vnewf, n_old, cd, vdf);
+  else
+    k_cross_scatter<double><<<g, 256, 0, s>>>(keys, ncross, xoff, rp_old, rp_all, erow, vnew, n_old, cd, vd);
+}
+
 }  // namespace vhci

@@ -107,6 +107,25 @@ void radix_sort_keys(uint64_t* keys, uint64_t* alt, int64_t n, int W, int nbits,
                      cudaStream_t s);
 
 // ---- Hamiltonian (k_ham.cu) ----
+// Incremental build (the stored rows of the first n_old states plus the rows of the nn states
+// appended since; H is symmetric to the bit).  hmerge_cross_keys: add[c] += 1 and a key
+// (c << 32 | e) for every new-row entry e in an old column c (cnt[0] counts the keys, in no fixed
+// order).  hmerge_entry_rows: erow[e] = the new row of entry e.  hmerge_lengths: merged row
+// lengths.  hmerge_copy_rows: rows [rs[i], rs[i+1]) to offset rd[i] (FP64 values, or FP32 when
+// vsf is given).  hmerge_cross_scatter: the sorted keys to the tails of the old rows (xoff:
+// exclusive scan of add).
+void hmerge_cross_keys(const int32_t* col_new, int64_t nnz_new, int64_t n_old, int32_t* add,
+                       uint64_t* keys, unsigned long long* cnt, cudaStream_t s);
+void hmerge_entry_rows(const int64_t* rp_new, int64_t nn, int32_t* erow, cudaStream_t s);
+void hmerge_lengths(const int64_t* rp_old, const int32_t* add, const int64_t* rp_new, int64_t n_old,
+                    int64_t nn, int32_t* len, cudaStream_t s);
+void hmerge_copy_rows(const int64_t* rs, const int32_t* cs, const double* vs, const float* vsf,
+                      int64_t nrows, const int64_t* rd, int32_t* cd, double* vd, float* vdf,
+                      cudaStream_t s);
+void hmerge_cross_scatter(const uint64_t* keys, int64_t ncross, const int64_t* xoff,
+                          const int64_t* rp_old, const int64_t* rp_all, const int32_t* erow,
+                          const double* vnew, const float* vnewf, int64_t n_old, int32_t* cd,
+                          double* vd, float* vdf, cudaStream_t s);
 // Rows row0 .. row0 + n - 1 of the Hamiltonian (rowcnt, rowptr, diag indexed from row0).
 void hbuild_count(const uint64_t* keys, int64_t row0, int64_t n, KeyLayout L, HashView basis,
                   ConnDev cd, int32_t* rowcnt, cudaStream_t s);
