@@ -553,10 +553,20 @@ int block_lanczos_impl(vhci_ctx* c, int k, bool dev_svqb) {
     // (theta_j, y_j) is W y_j[last block rows], so ||r_j||^2 = y_last^T (W^T W) y_last.  With the
     // full (two-pass) orthogonalisation the relation holds to rounding, far below the tolerance.
     // The whole space (m = n) or an invariant subspace (exhausted) leaves no residual.
-    const int pw = (!exhausted && m < n) ? p : 0;
+    // Mixed precision keeps the explicit residuals ||H x - theta x|| from the rotated products:
+    // its FP32-gather products carry rounding noise of about 1e-8 relative, and the Krylov relation
+    // (exact for the products as computed within one cycle) does not carry that noise across the
+    // restarts' coupling terms, so it can stall at the 1e-7 tolerance.
+    const int pw = (!exhausted && m < n && !mixed) ? p : 0;
     std::fill(rn.begin(), rn.end(), 0.0);
     VCK(d2h(c, th.data(), w.theta.p, nk * sizeof(double)));
-    if (pw > 0) {
+    if (mixed) {
+      VTRY(gemm_rows(c, w.HQ.p, ld, w.Yw.p, ld, nl, m, nk, 1.0, 0.0, w.HXb.p, kk));
+      residual_norms(w.Xb.p, w.HXb.p, nl, kk, nk, w.theta.p, w.part.p, nblk, w.rn2.p, s);
+      VTRY(comm_sum(c, w.rn2.p, nk));
+      VCK(d2h(c, rn.data(), w.rn2.p, nk * sizeof(double)));
+      VCK(cudaStreamSynchronize(s));
+    } else if (pw > 0) {
       copy_cols(w.HQ.p + (m - pw), ld, w.W.p, b, nl, pw, s);
       VCK(w.S.reserve((size_t)std::max(m, b) * pw, s));
       VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - pw) * ld, ld, nl, m, pw, w.W.p, b,
@@ -583,17 +593,31 @@ int block_lanczos_impl(vhci_ctx* c, int k, bool dev_svqb) {
       VCK(cudaStreamSynchronize(s));
     }
     const int keff = std::min(k, nk);
+    // Mixed precision measures the residual against the spectrum's scale (the largest |Ritz
+    // value| of this cycle) instead of |theta|: the FP32 gathers leave a noise floor proportional
+    // to ||H||, which a pair with small |theta| cannot get under; the FP64 sweep refines the pairs.
+    double scale = 0.0;
+    if (mixed) {
+      double tl = 0.0;
+      VCK(d2h(c, &tl, w.theta.p + (m - 1), sizeof(double)));
+      scale = std::max(std::fabs(th[0]), std::fabs(tl));
+    }
+    auto thresh = [&](int j) { return tol * std::max({eps23, std::fabs(th[j]), scale}); };
     int nconv = 0;
     double rmax = 0.0;
     for (int j = 0; j < keff; ++j) {
       const double r = std::sqrt(std::max(rn[j], 0.0));
       rmax = std::max(rmax, r);
-      if (r <= tol * std::max(eps23, std::fabs(th[j]))) ++nconv;
+      if (r <= thresh(j)) ++nconv;
     }
     t_rr += msince(t0);
     if (plevel >= 2)
       std::fprintf(stderr, "  lanczos cycle %d m %d b %d converged %d/%d max|r| %.3e\n", cyc, m, b,
                    nconv, keff, rmax);
+    if (plevel >= 3)
+      for (int j = 0; j < keff; ++j)
+        if (!(std::sqrt(std::max(rn[j], 0.0)) <= thresh(j)))
+          std::fprintf(stderr, "    pair %d theta %.10e |r|^2 %.3e\n", j, th[j], rn[j]);
     if (nconv == keff || m >= n || exhausted) {
       if (nconv < keff && !(m >= n || exhausted))
         return fail(c, VHCI_E_NOT_CONVERGED, "Error: Eigenvalues did not converge.");
@@ -605,8 +629,17 @@ int block_lanczos_impl(vhci_ctx* c, int k, bool dev_svqb) {
       w.release(s);
       return VHCI_OK;
     }
-    // ---- thick restart: keep the Ritz block, continue from the pending block W formed above
+    // ---- thick restart: keep the Ritz block, continue from the pending block W (formed above
+    // with the residuals, or here in mixed precision, whose rotated products are kept with it)
     t0 = now();
+    if (mixed) {
+      copy_cols(w.HQ.p + (m - p), ld, w.W.p, b, nl, p, s);
+      VCK(w.S.reserve((size_t)std::max(m, b) * p, s));
+      VTRY(gemm_rows_gram(c, w, w.Q.p, ld, w.T.p + (size_t)(m - p) * ld, ld, nl, m, p, w.W.p, b,
+                          w.S.p, m));
+      VTRY(gemm_rows(c, w.Q.p, ld, w.S.p, m, nl, m, p, -1.0, 1.0, w.W.p, b));
+      copy_cols(w.HXb.p, kk, w.HQ.p, ld, nl, nk, s);
+    }
     copy_cols(w.Xb.p, kk, w.Q.p, ld, nl, nk, s);
     int p2 = p;
     if (dev) VTRY(svqb_dev(c, w, nl, w.W.p, b, p, w.Q.p + nk, ld));
