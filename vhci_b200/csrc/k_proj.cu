@@ -126,8 +126,9 @@ inline int gram_groups(int Mc, int tiles_per_warp, int nwarp) {
 // Sums the blocks' partials: a block of kRedWarps warps owns 32 consecutive entries of C; warp w
 // adds the partials of blocks w, w + kRedWarps, ... (lane = entry, so each partial row is read as
 // one 256-byte segment) and the warps' sums are combined in warp order, so the result is the same
-// on every run.
-constexpr int kRedWarps = 8;
+// on every run.  32 warps: a narrow product leaves thousands of partials (148 blocks x 16 row
+// groups) for few entries of C.
+constexpr int kRedWarps = 32;
 __global__ void __launch_bounds__(kRedWarps * 32) k_gram_reduce(const double* __restrict__ part,
                                                                 int nblk, int M, int P, double alpha,
                                                                 double beta, double* __restrict__ C,
@@ -362,24 +363,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_rows_gram(const double* __restr
   }
 }
 
-// SVQB factor of a small Gram matrix on the device (one warp), so that a Lanczos step needs no
-// host round trip.  S (nb x nb, column-major, nb <= 16) = W^T W.  With D = diag(S)^(-1/2) (zero for
-// a diagonal at or below 1e-28 of the largest), D S D = U L U^T by cyclic Jacobi in the parallel
-// round-robin order (nb/2 disjoint rotations per round, Golub-Van Loan's symmetric 2 x 2 Schur
-// step, at most 30 sweeps, stop when the off-diagonal square sum is below 1e-30 of the total);
-// the directions with L > 1e-12 max(L) are kept in descending order and
+// SVQB factor of a small Gram matrix on the device (one block of 128 threads), so that a Lanczos
+// step needs no host round trip.  S (nb x nb, column-major, nb <= 16) = W^T W.  With
+// D = diag(S)^(-1/2) (zero for a diagonal at or below 1e-28 of the largest), D S D = U L U^T by
+// cyclic Jacobi in the parallel round-robin order (nb/2 disjoint rotations per round, Golub-Van
+// Loan's symmetric 2 x 2 Schur step; one thread per (rotation, row) update), at most 30 sweeps,
+// stopping when every off-diagonal |a_ij| <= 1e-14 sqrt(a_ii a_jj) among the directions above
+// 1e-12 of the largest (the relative test bounds the orthonormality of W M independently of the
+// block's conditioning); the directions with L > 1e-12 max(L) are kept in descending order and
 // M[:, q] = D U[:, keep_q] / sqrt(L[keep_q]) (columns past the rank are zero).  W M is then
 // orthonormal.  *rank_short is set to 1 when fewer than nb directions are kept.
-__global__ void __launch_bounds__(32) k_svqb_factor(const double* __restrict__ S, int nb,
-                                                    double* __restrict__ M,
-                                                    int* __restrict__ rank_short) {
-  __shared__ double A[16][17], U[16][17], d[16], cs[8], sn[8];
+constexpr int kSvqbThreads = 128;
+__global__ void __launch_bounds__(kSvqbThreads) k_svqb_factor(const double* __restrict__ S, int nb,
+                                                              double* __restrict__ M,
+                                                              int* __restrict__ rank_short) {
+  __shared__ double A[16][17], U[16][17], d[16], cs[8], sn[8], red[kSvqbThreads / 32];
   __shared__ int pa[8], pb[8], keep[16];
   __shared__ int stop, rr;
-  const int lane = threadIdx.x;
-  for (int x = lane; x < nb * nb; x += 32) A[x % nb][x / nb] = S[x];
-  __syncwarp();
-  if (lane == 0) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int x = tid; x < nb * nb; x += kSvqbThreads) A[x % nb][x / nb] = S[x];
+  __syncthreads();
+  if (tid == 0) {
     double dmax = 0.0;
     for (int i = 0; i < nb; ++i) dmax = fmax(dmax, A[i][i]);
     for (int i = 0; i < nb; ++i) {
@@ -387,55 +391,65 @@ __global__ void __launch_bounds__(32) k_svqb_factor(const double* __restrict__ S
       d[i] = (v > 1e-28 * dmax && v > 1e-300) ? 1.0 / sqrt(v) : 0.0;
     }
   }
-  __syncwarp();
-  for (int x = lane; x < nb * nb; x += 32) {
-    const int i = x % nb, j = x / nb;
-    A[i][j] *= d[i] * d[j];
-    U[i][j] = i == j ? 1.0 : 0.0;
+  __syncthreads();
+  for (int x = tid; x < 256; x += kSvqbThreads) {
+    const int i = x & 15, j = x >> 4;
+    if (i < nb && j < nb) {
+      A[i][j] *= d[i] * d[j];
+      U[i][j] = i == j ? 1.0 : 0.0;
+    }
   }
-  __syncwarp();
+  __syncthreads();
   const int N = (nb + 1) & ~1;  // players of the round-robin (one idle index when nb is odd)
   for (int sweep = 0; sweep < 30; ++sweep) {
-    if (lane == 0) {
-      double off = 0.0, tot = 0.0;
-      for (int j = 0; j < nb; ++j)
-        for (int i = 0; i < nb; ++i) {
-          tot += A[i][j] * A[i][j];
-          if (i != j) off += A[i][j] * A[i][j];
-        }
-      stop = (off <= 1e-30 * tot || off == 0.0) ? 1 : 0;
+    // relative off-diagonal size over the directions that count
+    double dmx = 0.0;
+    for (int i = 0; i < nb; ++i) dmx = fmax(dmx, A[i][i]);
+    double mr = 0.0;
+    for (int x = tid; x < 256; x += kSvqbThreads) {
+      const int i = x & 15, j = x >> 4;
+      if (i < j && j < nb && A[i][i] > 1e-12 * dmx && A[j][j] > 1e-12 * dmx)
+        mr = fmax(mr, fabs(A[i][j]) / sqrt(A[i][i] * A[j][j]));
     }
-    __syncwarp();
+    for (int o = 16; o > 0; o >>= 1) mr = fmax(mr, __shfl_xor_sync(~0u, mr, o));
+    if (lane == 0) red[wid] = mr;
+    __syncthreads();
+    if (tid == 0) {
+      double m = 0.0;
+      for (int w = 0; w < kSvqbThreads / 32; ++w) m = fmax(m, red[w]);
+      stop = m <= 1e-14 ? 1 : 0;
+    }
+    __syncthreads();
     if (stop) break;
     for (int round = 0; round < N - 1; ++round) {
-      if (lane < N / 2) {
-        int a = lane == 0 ? N - 1 : (lane + round) % (N - 1);
-        int b = lane == 0 ? round % (N - 1) : (N - 1 - lane + round) % (N - 1);
+      if (tid < N / 2) {
+        int a = tid == 0 ? N - 1 : (tid + round) % (N - 1);
+        int b = tid == 0 ? round % (N - 1) : (N - 1 - tid + round) % (N - 1);
         if (a > b) { const int t = a; a = b; b = t; }
-        double c = 1.0, sgn = 0.0;
+        double c = 1.0, sg = 0.0;
         if (b < nb) {
           const double apq = A[a][b];
           if (fabs(apq) >= 1e-300) {
             const double theta = (A[b][b] - A[a][a]) / (2.0 * apq);
             const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
             c = 1.0 / sqrt(t * t + 1.0);
-            sgn = t * c;
+            sg = t * c;
           }
         }
-        pa[lane] = a; pb[lane] = b; cs[lane] = c; sn[lane] = sgn;
+        pa[tid] = a; pb[tid] = b; cs[tid] = c; sn[tid] = sg;
       }
-      __syncwarp();
-      for (int x = lane; x < (N / 2) * nb; x += 32) {  // rows a, b
-        const int t = x / nb, k = x % nb, a = pa[t], b = pb[t];
-        if (b >= nb) continue;
+      __syncthreads();
+      const int t = tid >> 4, k = tid & 15;  // rotation t, row / column k
+      const bool on = t < N / 2 && k < nb && pb[t] < nb;
+      if (on) {  // rows a, b
+        const int a = pa[t], b = pb[t];
         const double ra = A[a][k], rb = A[b][k];
         A[a][k] = cs[t] * ra - sn[t] * rb;
         A[b][k] = sn[t] * ra + cs[t] * rb;
       }
-      __syncwarp();
-      for (int x = lane; x < (N / 2) * nb; x += 32) {  // columns a, b of A and U
-        const int t = x / nb, k = x % nb, a = pa[t], b = pb[t];
-        if (b >= nb) continue;
+      __syncthreads();
+      if (on) {  // columns a, b of A and U
+        const int a = pa[t], b = pb[t];
         const double ca = A[k][a], cb = A[k][b];
         A[k][a] = cs[t] * ca - sn[t] * cb;
         A[k][b] = sn[t] * ca + cs[t] * cb;
@@ -443,10 +457,10 @@ __global__ void __launch_bounds__(32) k_svqb_factor(const double* __restrict__ S
         U[k][a] = cs[t] * ua - sn[t] * ub;
         U[k][b] = sn[t] * ua + cs[t] * ub;
       }
-      __syncwarp();
+      __syncthreads();
     }
   }
-  if (lane == 0) {
+  if (tid == 0) {
     // descending eigenvalues above 1e-12 of the largest
     int ord[16];
     for (int i = 0; i < nb; ++i) ord[i] = i;
@@ -463,8 +477,8 @@ __global__ void __launch_bounds__(32) k_svqb_factor(const double* __restrict__ S
     rr = r;
     if (r < nb) *rank_short = 1;
   }
-  __syncwarp();
-  for (int x = lane; x < nb * nb; x += 32) {
+  __syncthreads();
+  for (int x = tid; x < nb * nb; x += kSvqbThreads) {
     const int i = x % nb, q = x / nb;
     M[x] = q < rr ? d[i] * U[i][keep[q]] / sqrt(A[keep[q]][keep[q]]) : 0.0;
   }
@@ -492,7 +506,7 @@ void set_attributes() {
 
 void svqb_factor(const double* S, int nb, double* M, int* rank_short, cudaStream_t s) {
   note_launch();
-  k_svqb_factor<<<1, 32, 0, s>>>(S, nb, M, rank_short);
+  k_svqb_factor<<<1, kSvqbThreads, 0, s>>>(S, nb, M, rank_short);
 }
 
 int64_t proj_gram_scratch(int M, int P) {
